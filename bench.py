@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""bench.py -- zone-cycles/s of the HOW-MHD time step on B200.
+
+Workload (the headline configuration): 3-D MHD blast, 256^3 periodic cube,
+rho = 1, p = 10 inside r < 0.1 and 0.1 outside, B = (1, 1, 0)/sqrt 2, gam 5/3,
+cour 0.4, floors 1e-6 (problem `blast3d_b`).  One bench step = one CFL
+reduction (tstep) + one SSPRK(5,4) step (5 stages x 3 fused WENO sweeps + CT +
+prot + ghost fills) over the whole domain; 1 zone-cycle = one active zone
+advanced by one step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--n 256] [--precision fp64|mixed]
+
+`value` is device-timed with inputs resident in HBM; `e2e` goes through the
+C ABI with host (pinned) buffers: upload q + face B, tstep, ssprk, download,
+every step.  Under torchrun each rank advances its own replica (the path has
+no data exchange at one domain per GPU), time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "how-mhd-kokkos_b200"))
+
+METRIC = "zone-cycles/s, 256^3 blast: plain FP64 vs mixed+learned, same L1 err, 1 B200"
+UNIT = "zone-cycles/s"
+# Algorithmic FP64 operations (add/sub/mul/div/sqrt/max/abs = 1 each), counted
+# by instantiating the CPU restatement's cell/interface kernels on a counting
+# scalar: 3,088 per zone per directional sweep (primitives 21, centre 71,
+# interface eigenvectors 527, 7 x WENO field 332, 7 x back-projection 14,
+# 7 x update 3, CT terms 26); per zone-cycle 5 x (3 x 3,088 + RK 46 + CT 147
+# + prot 25) + stage-5 base 48 + tstep 60 = 47,518.
+SWEEP_FLOP_PER_ZONE = 3088
+FLOP_PER_ZONE_CYCLE = 47518
+REF_SAMPLE_N = 64
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload_text(n, precision, tend=1.0e3):
+    # tend far beyond the timed steps so no step is shortened by the output clamp
+    return (f"nx {n}\nny {n}\nnz {n}\nnt 1\ntend {tend!r}\ngam 1.6666666666666667\ncour 0.4\n"
+            f"problem blast3d_b\nx1bc periodic\nx2bc periodic\nx3bc periodic\n"
+            f"rhomin 1e-6\npgmin 1e-6\nprecision {precision}\n")
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_id):
+        self.dev_id = dev_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev_id}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, smax, reasons = [], [], set()
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def device_id_for_smi(local):
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:   # noqa: BLE001
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        return vis.split(",")[local] if vis else str(local)
+
+
+# -------------------------------------------------------------- CPU baseline
+def ref_binary():
+    b = REPO / "oracle" / "_ref" / "how_ref"
+    return b if b.exists() else None
+
+
+def run_reference_sample(steps, warmup, threads):
+    """Time the reference's own CPU path (oracle/_ref/how_ref) on the 64^3 sample;
+    returns (zone-cycles/s, kind, sample description).  Falls back to the oracle
+    port (oracle/_build/liboracle.so) when the reference build is absent."""
+    import numpy as np
+    import how_mhd as hm
+    n = REF_SAMPLE_N
+    sample = (f"blast3d_b {n}^3 (the headline problem at a size the host finishes in seconds), "
+              f"{steps} timed SSPRK step(s) after {warmup} warm-up, {threads} OpenMP threads")
+    text = workload_text(n, "fp64")
+    p = hm.read_parameters(text)
+    q = hm.problem_state(p)
+    binp = ref_binary()
+    if binp is not None:
+        sys.path.insert(0, str(REPO / "tests"))
+        from howtest import write_dump
+        with tempfile.TemporaryDirectory() as td:
+            inp = Path(td) / "in.txt"
+            inp.write_text(text)
+            st = Path(td) / "state.bin"
+            write_dump(st, {"q": q})
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            r = subprocess.run([str(binp), str(inp), "/dev/null", "--state", str(st), "--steps", str(steps),
+                                "--warmup", str(warmup), "--time-only", "--threads", str(threads)],
+                               capture_output=True, text=True, env=env, timeout=3600)
+            if r.returncode == 0:
+                js = json.loads(r.stdout.strip().splitlines()[-1])
+                return js["zone_cycles_per_s"], "reference", sample
+    # oracle port
+    sys.path.insert(0, str(REPO / "tests"))
+    from howtest import CPUOracle, oracle_lib
+    oracle_lib().oracle_set_threads(threads)
+    o = CPUOracle(n, n, n, gam=5.0 / 3.0, rhomin=1e-6, pgmin=1e-6)
+    o.set_state(q)
+    for _ in range(warmup):
+        o.ssprk(o.tstep())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.ssprk(o.tstep())
+    el = time.perf_counter() - t0
+    return n ** 3 * steps / el, "port", sample.replace("OpenMP", "OpenMP (oracle port)")
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- reference arm
+def bench_reference(args):
+    world, rank, local = dist_info()
+    if rank != 0:
+        return 0
+    threads = host_threads()
+    t0 = time.perf_counter()
+    zcs, kind, sample = run_reference_sample(max(args.steps, 1), args.warmup, threads)
+    n3 = REF_SAMPLE_N ** 3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": zcs, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n3 / zcs,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"3-D MHD blast (blast3d_b) {REF_SAMPLE_N}^3 sample of the 256^3 workload, "
+                               "reference Kokkos/OpenMP path built from its own sources"},
+        "cpu_baseline": {"value": zcs, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": zcs, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def load_traffic_profile(precision):
+    f = REPO / "profiles" / "sweep_traffic.json"
+    if not f.exists():
+        return None
+    try:
+        d = json.loads(f.read_text())
+        return d.get(precision, d.get("fp64"))
+    except Exception:   # noqa: BLE001
+        return None
+
+
+def bench_ours(args):
+    import numpy as np
+    import torch
+    import how_mhd as hm
+
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    n = args.n
+    p = hm.read_parameters(workload_text(n, args.precision))
+    dom = hm.Domain(p)
+    dom.init_problem()
+    stream = torch.cuda.ExternalStream(dom.stream)
+
+    fp64_peak = ctypes_peak(hm)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    t_sim, s, _ = dom.run(0.0, args.warmup)
+    barrier()
+    sampler = ClockSampler(device_id_for_smi(local)) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.5)
+    hm.lib().how_set_kernel_timing(dom._h, 1)
+    l0 = dom.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    t_sim, s, _ = dom.run(t_sim, args.steps)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = dom.kernel_launches - l0
+    import ctypes
+    sweep_ms = ctypes.c_double()
+    sweep_n = ctypes.c_long()
+    hm.lib().how_get_kernel_timing(dom._h, ctypes.byref(sweep_ms), ctypes.byref(sweep_n))
+    hm.lib().how_set_kernel_timing(dom._h, 0)
+    clocks = sampler.stop() if sampler else None
+    ms = max_over_ranks(ms)
+    value = world * n ** 3 * args.steps / (ms * 1e-3)
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        shp = (8,) + tuple(p.shape)
+        qh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
+        bh = [torch.empty(tuple(p.shape), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+        dom.get_state(0, out=qh)
+        dom.get_face_b_into(*bh)
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            dom.set_state(qh)
+            dom.set_face_b(*bh)
+            dt = dom.tstep()
+            dom.ssprk(dt)
+            dom.get_state(0, out=qh)
+            dom.get_face_b_into(*bh)
+        f1.record(stream)
+        barrier()
+        ems = max_over_ranks(f0.elapsed_time(f1))
+        nbytes = 8 * int(np.prod(shp)) + 3 * 8 * int(np.prod(p.shape))
+        e2e = {"value": world * n ** 3 * args.steps / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "ms_per_step": ems / args.steps}
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    avg_sweep_ms = sweep_ms.value / max(sweep_n.value, 1)
+    achieved = SWEEP_FLOP_PER_ZONE * n ** 3 / (avg_sweep_ms * 1e-3) / 1e12
+    traffic = None
+    tp = load_traffic_profile(args.precision)
+    if tp and "dram_bytes_per_zone" in tp:
+        traffic = tp["dram_bytes_per_zone"] * n ** 3
+    roofline = {
+        "bound": "fp64", "unit": "TFLOP/s", "kernel": "k_sweep (fused directional WENO sweep)",
+        "achieved": achieved, "peak": fp64_peak, "frac": achieved / fp64_peak if fp64_peak else None,
+        "peak_source": "measured live: FP64 FMA-pipe probe (how_measure_fp64_peak), of measured",
+        "flop_per_launch": SWEEP_FLOP_PER_ZONE * n ** 3, "avg_launch_ms": avg_sweep_ms,
+        "launches_timed": sweep_n.value, "share_of_step": sweep_ms.value / ms if ms else None,
+        "traffic": traffic,
+        "step_frac": value / world * FLOP_PER_ZONE_CYCLE / (fp64_peak * 1e12) if fp64_peak else None,
+    }
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        threads = host_threads()
+        zcs, kind, sample = run_reference_sample(1, 1, threads)
+        cpu = {"value": zcs, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": f"3-D MHD blast {n}^3 (blast3d_b), periodic, gam 5/3, cour 0.4, floors 1e-6; "
+                               f"SSPRK(5,4) + characteristic WENO5/LLF + 4th-order CT",
+                   "n": n, "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "state 12.5 GB per replica >> 126 MB L2: every step streams from HBM, no flush"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ctypes_peak(hm):
+    import ctypes
+    v = ctypes.c_double()
+    rc = hm.lib().how_measure_fp64_peak(ctypes.byref(v), 5)
+    return v.value if rc == 0 else None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,127 @@
+// how_internal.cuh -- device-side geometry, context and kernel entry points
+// shared by the translation units of libhowmhd.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "how_mhd.h"
+
+namespace how {
+
+// Device layout: one padded 3-D array ("field") per (stage, variable), x
+// fastest.  Index (i, j, k) -> (k * P1 + j) * pitch + i with i,j,k in the
+// reference's padded ranges [0, n+6).  pitch >= P0 and a multiple of 8 so
+// every row starts on a 64-byte boundary; fields are 256-byte aligned.
+struct Grid {
+    int nx, ny, nz;
+    int P0, P1, P2;
+    int pitch;
+    long long fs;   // doubles between consecutive fields
+    __host__ __device__ inline long long idx(int i, int j, int k) const {
+        return ((long long)k * P1 + j) * pitch + i;
+    }
+};
+
+inline Grid make_grid(int nx, int ny, int nz) {
+    Grid g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.P0 = nx + 6; g.P1 = ny + 6; g.P2 = nz + 6;
+    g.pitch = (g.P0 + 7) / 8 * 8;
+    long long f = (long long)g.pitch * g.P1 * g.P2;
+    g.fs = (f + 31) / 32 * 32;
+    return g;
+}
+
+// SSPRK(5,4) coefficients (src/ssprk.cpp:66-94)
+struct RKCoeff { double k1, k2, k3, k4, k5; };
+inline RKCoeff rk_coeff(int iw) {
+    switch (iw) {
+        case 1: return {1.0, 0.39175222700392, 0.0, 0.0, 0.0};
+        case 2: return {0.44437049406734, 0.36841059262959, 0.55562950593266, 0.0, 0.0};
+        case 3: return {0.62010185138540, 0.25189177424738, 0.37989814861460, 0.0, 0.0};
+        case 4: return {0.17807995410773, 0.54497475021237, 0.82192004589227, 0.0, 0.0};
+        default: return {-2.081261929715610e-02, 0.22600748319395, 5.03580947213895e-1,
+                         0.51723167208978, -6.518979800418380e-12};
+    }
+}
+
+// Device scalars of a context (one cache line each group).
+struct DevScalars {
+    unsigned long long vmax_bits[3];   // tstep reduction (max of non-negative doubles)
+    unsigned int status;               // HOW_STATUS_* bits set by kernels
+    unsigned int pad0;
+    double dt;                         // current step's dt
+    double dtdl[6][3];                 // k2(iw) * dt / d(x,y,z), iw = 1..5
+    double dt_raw;                     // dt before the output-time clamp
+};
+
+enum : unsigned int { HOW_STATUS_NONFINITE_DT = 1u };
+
+// Arguments of one directional sweep launch.
+struct SweepArgs {
+    Grid g;
+    const double* qprev;   // stage iw-1, field 0 (vars at + v * fs)
+    double* qout;          // stage iw
+    const double* q0;      // stage 0 (RK base)
+    const double* q2;      // stage 2 (stage-5 base only)
+    const double* q3;      // stage 3 (stage-5 base only)
+    double* cta;           // CT flux array fed by the B_t1 row
+    double* ctb;           // CT flux array fed by the B_t2 row
+    const double* dtdl;    // device: k2 * dt / d_dir for this stage
+    double k1, k3, c4, c5; // c4 = k4 / k1, c5 = k5 / k1
+    int mode;              // 0 accumulate, 1 first sweep with RK combine, 2 first sweep base+delta
+    int stage5;            // base = q0 + c4 q2 + c5 q3
+    double gam, rhomin, pgmin;
+};
+
+struct Ctx {
+    how_params p;
+    Grid g;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    double* mem = nullptr;          // one allocation for every field
+    size_t mem_bytes = 0;
+    double* q[6] = {};              // stage s, field 0; var v at + v * fs
+    double* b[6] = {};              // face B stage s: comps at + c * fs
+    double* ct[12] = {};            // fsy fsz gsx gsz hsx hsy Ox2 Oy2 Oz2 Ox Oy Oz
+    double* stage_buf = nullptr;    // device staging for layout conversion (8 fields)
+    DevScalars* dsc = nullptr;      // device scalars
+    DevScalars* hsc = nullptr;      // pinned host mirror
+    long launches = 0;
+    int precision = HOW_PREC_FP64;
+    bool have_state = false;
+};
+
+// ---- kernels / launchers (defined in the .cu files) ------------------------
+void launch_ref_to_dev(Ctx& c, const double* ref_dev, double* dst, int nvar);
+void launch_dev_to_ref(Ctx& c, const double* src, double* ref_dev, int nvar);
+void launch_bound(Ctx& c, double* const* fields, int nfields);
+void launch_init_faceb(Ctx& c);
+void launch_tstep(Ctx& c, double time, double target, int clamp);
+void launch_set_dt(Ctx& c);     // dt already in dsc->dt: fill dtdl
+void launch_sweep(Ctx& c, int dir, const SweepArgs& a);
+void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5);
+void launch_faceb_base(Ctx& c, int iw, double c4, double c5, int stage5);
+void launch_prot(Ctx& c, int stage);
+void launch_copy_fields(Ctx& c, double* dst, const double* src, int nfields);
+
+void set_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+
+// event timing of kernel launches (instrument.cu)
+void timer_begin(Ctx& c, cudaEvent_t* pair_out);
+void timer_end(Ctx& c, cudaEvent_t* pair);
+
+}  // namespace how
+
+// The opaque handle of the C ABI is the context itself.
+struct how_ctx : how::Ctx {};
+
+#define HOW_CUDA_CHECK(expr)                                   \
+    do {                                                       \
+        cudaError_t e_ = (expr);                               \
+        if (e_ != cudaSuccess) return how::cuda_fail(e_, #expr); \
+    } while (0)

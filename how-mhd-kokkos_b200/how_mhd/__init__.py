@@ -1,0 +1,330 @@
+"""how_mhd -- Python mirror of the HOW-MHD driver-level interface over the C ABI
+of libhowmhd.so (include/how_mhd.h).
+
+The functions keep the reference's names and argument meaning
+(jeongbhin/HOW-MHD-Kokkos: read_parameters, init_problem, bound,
+bound_bfield, initialize_bfield_from_q, tstep, ssprk, prot, register_problem)
+with a device-resident `Domain` in place of the Kokkos View `q` and the
+module-global face-B arrays.  Errors raise `HowError` carrying the C status and
+message; nothing aborts.  The CUDA library is required: importing this module
+without libhowmhd.so raises ImportError (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIBPATH = Path(os.environ.get("HOW_MHD_LIB", _HERE.parent / "libhowmhd.so"))
+
+HOW_OK = 0
+HOW_BC_PERIODIC, HOW_BC_OPEN = 0, 1
+HOW_PREC_FP64, HOW_PREC_MIXED = 0, 1
+_ERRNAMES = {-1: "ARG", -2: "PARSE", -3: "PROBLEM", -4: "CUDA", -5: "NODEVICE",
+             -6: "NONFINITE", -7: "DT", -8: "STATE"}
+
+
+class HowError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"HOW_ERR_{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    """struct how_params (include/how_mhd.h), i.e. the reference's Parameters."""
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("nt", ctypes.c_int), ("nstep", ctypes.c_int), ("ntime", ctypes.c_int),
+        ("xsize", ctypes.c_double), ("ysize", ctypes.c_double), ("zsize", ctypes.c_double),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("gam", ctypes.c_double), ("cour", ctypes.c_double), ("tend", ctypes.c_double),
+        ("rhomin", ctypes.c_double), ("pgmin", ctypes.c_double),
+        ("bc", ctypes.c_int * 3),
+        ("px", ctypes.c_int), ("py", ctypes.c_int), ("pz", ctypes.c_int),
+        ("problem", ctypes.c_char * 64),
+        ("output_format", ctypes.c_char * 16),
+        ("precision", ctypes.c_int),
+        ("router", ctypes.c_int),
+        ("seed", ctypes.c_uint64),
+        ("problem_par", ctypes.c_double * 8),
+    ]
+
+    @property
+    def shape(self):
+        return (self.nx + 6, self.ny + 6, self.nz + 6)
+
+
+PROBLEM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(Params), ctypes.c_void_p)
+
+
+def _load():
+    if not _LIBPATH.exists():
+        raise ImportError(f"libhowmhd.so not found at {_LIBPATH}; build it with "
+                          f"`make -C {_HERE.parent}` (CUDA sm_100a); there is no CPU fallback")
+    lib = ctypes.CDLL(str(_LIBPATH))
+    D = ctypes.POINTER(ctypes.c_double)
+    P = ctypes.POINTER(Params)
+    V = ctypes.c_void_p
+    sig = {
+        "how_params_default": ([P], ctypes.c_int),
+        "how_parse_input": ([ctypes.c_char_p, P], ctypes.c_int),
+        "how_parse_input_string": ([ctypes.c_char_p, P], ctypes.c_int),
+        "how_finalize_params": ([P], ctypes.c_int),
+        "how_register_problem": ([ctypes.c_char_p, PROBLEM_FN, V], ctypes.c_int),
+        "how_list_problems": ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "how_problem_init_host": ([P, D], ctypes.c_int),
+        "how_create": ([P, ctypes.POINTER(V)], ctypes.c_int),
+        "how_destroy": ([V], ctypes.c_int),
+        "how_last_error": ([], ctypes.c_char_p),
+        "how_get_params": ([V, P], ctypes.c_int),
+        "how_device_bytes": ([V], ctypes.c_size_t),
+        "how_init_problem": ([V], ctypes.c_int),
+        "how_set_state": ([V, ctypes.c_int, D], ctypes.c_int),
+        "how_get_state": ([V, ctypes.c_int, D], ctypes.c_int),
+        "how_set_face_b": ([V, ctypes.c_int, D, D, D], ctypes.c_int),
+        "how_get_face_b": ([V, ctypes.c_int, D, D, D], ctypes.c_int),
+        "how_bound": ([V, ctypes.c_int], ctypes.c_int),
+        "how_bound_bfield": ([V, ctypes.c_int], ctypes.c_int),
+        "how_init_bfield_from_q": ([V], ctypes.c_int),
+        "how_tstep": ([V, D], ctypes.c_int),
+        "how_ssprk": ([V, ctypes.c_double], ctypes.c_int),
+        "how_prot": ([V, ctypes.c_int], ctypes.c_int),
+        "how_sweep": ([V, ctypes.c_int, ctypes.c_double], ctypes.c_int),
+        "how_get_ct_array": ([V, ctypes.c_int, D], ctypes.c_int),
+        "how_run": ([V, D, ctypes.c_long, ctypes.POINTER(ctypes.c_long), D, ctypes.c_long], ctypes.c_int),
+        "how_set_precision": ([V, ctypes.c_int], ctypes.c_int),
+        "how_sync": ([V], ctypes.c_int),
+        "how_kernel_launches": ([V], ctypes.c_long),
+        "how_stream": ([V], ctypes.c_void_p),
+        "how_set_kernel_timing": ([V, ctypes.c_int], ctypes.c_int),
+        "how_get_kernel_timing": ([V, D, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
+        "how_measure_fp64_peak": ([D, ctypes.c_int], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+_lib = _load()
+LIBRARY_PATH = str(_LIBPATH)
+
+
+def _check(rc):
+    if rc != HOW_OK:
+        raise HowError(rc, _lib.how_last_error().decode(errors="replace"))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def lib():
+    """The loaded ctypes library (for instrumentation)."""
+    return _lib
+
+
+# --------------------------------------------------------------- parameters
+def default_parameters() -> Params:
+    p = Params()
+    _check(_lib.how_params_default(ctypes.byref(p)))
+    return p
+
+
+def read_parameters(source) -> Params:
+    """read_parameters + finalize_parameters_after_read (src/parameters.cpp:7-160).
+
+    `source` is a path to an input.in file or the text itself (contains a newline)."""
+    p = Params()
+    if isinstance(source, (str, os.PathLike)) and "\n" not in str(source) and Path(source).exists():
+        _check(_lib.how_parse_input(str(source).encode(), ctypes.byref(p)))
+    else:
+        _check(_lib.how_parse_input_string(str(source).encode(), ctypes.byref(p)))
+    return p
+
+
+def make_parameters(**kw) -> Params:
+    """Parameters from keywords using the input.in key names (bc as strings)."""
+    lines = []
+    for k, v in kw.items():
+        lines.append(f"{k} {v!r}" if isinstance(v, float) else f"{k} {v}")
+    return read_parameters("\n".join(lines) + "\n")
+
+
+# ------------------------------------------------------------------ problems
+_registered_callbacks = []
+
+
+def register_problem(name: str, fn) -> None:
+    """register_problem (src/problem.hpp:8-22).  fn(q, params) fills one stage of q
+    (numpy array (8, nx+6, ny+6, nz+6), reference layout) in place."""
+    def cb(qptr, pptr, user):
+        try:
+            p = pptr.contents
+            q = np.ctypeslib.as_array(qptr, shape=(8,) + p.shape)
+            fn(q, p)
+            return 0
+        except Exception:   # noqa: BLE001 -- reported as a C status
+            return 1
+    c = PROBLEM_FN(cb)
+    _registered_callbacks.append(c)
+    _check(_lib.how_register_problem(name.encode(), c, None))
+
+
+def list_problems():
+    buf = ctypes.create_string_buffer(1 << 14)
+    _lib.how_list_problems(buf, len(buf))
+    return [s for s in buf.value.decode().split("\n") if s]
+
+
+def problem_state(params: Params) -> np.ndarray:
+    """init_problem on the host: stage 0 of q in the reference layout."""
+    q = np.zeros((8,) + params.shape)
+    _check(_lib.how_problem_init_host(ctypes.byref(params), _dptr(q)))
+    return q
+
+
+# -------------------------------------------------------------------- domain
+class Domain:
+    """Device-resident q(6 stages) + face B + CT arrays of one run (how_ctx)."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        h = ctypes.c_void_p()
+        _check(_lib.how_create(ctypes.byref(params), ctypes.byref(h)))
+        self._h = h
+        p = Params()
+        _check(_lib.how_get_params(h, ctypes.byref(p)))
+        self.params = p
+        self.shape = p.shape
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.how_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # state
+    def set_state(self, q, stage=0):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        if q.shape != (8,) + self.shape:
+            raise ValueError(f"state shape {q.shape} != {(8,) + self.shape}")
+        _check(_lib.how_set_state(self._h, stage, _dptr(q)))
+
+    def get_state(self, stage=0, out=None):
+        q = out if out is not None else np.empty((8,) + self.shape)
+        _check(_lib.how_get_state(self._h, stage, _dptr(q)))
+        return q
+
+    def set_face_b(self, bx, by, bz, stage=0):
+        arrs = [np.ascontiguousarray(b, dtype=np.float64) for b in (bx, by, bz)]
+        _check(_lib.how_set_face_b(self._h, stage, *(_dptr(a) for a in arrs)))
+
+    def get_face_b(self, stage=0):
+        b = [np.empty(self.shape) for _ in range(3)]
+        _check(_lib.how_get_face_b(self._h, stage, *(_dptr(x) for x in b)))
+        return b
+
+    def get_face_b_into(self, bx, by, bz, stage=0):
+        for x in (bx, by, bz):
+            if x.shape != self.shape or x.dtype != np.float64 or not x.flags.c_contiguous:
+                raise ValueError("face-B buffers must be C-contiguous float64 of the padded shape")
+        _check(_lib.how_get_face_b(self._h, stage, _dptr(bx), _dptr(by), _dptr(bz)))
+
+    def get_ct_array(self, which):
+        a = np.empty(self.shape)
+        _check(_lib.how_get_ct_array(self._h, which, _dptr(a)))
+        return a
+
+    # path functions
+    def init_problem(self):
+        _check(_lib.how_init_problem(self._h))
+
+    def bound(self, stage):
+        _check(_lib.how_bound(self._h, stage))
+
+    def bound_bfield(self, stage):
+        _check(_lib.how_bound_bfield(self._h, stage))
+
+    def initialize_bfield_from_q(self):
+        _check(_lib.how_init_bfield_from_q(self._h))
+
+    def tstep(self) -> float:
+        dt = ctypes.c_double()
+        _check(_lib.how_tstep(self._h, ctypes.byref(dt)))
+        return dt.value
+
+    def ssprk(self, dt: float):
+        _check(_lib.how_ssprk(self._h, dt))
+
+    def prot(self, stage):
+        _check(_lib.how_prot(self._h, stage))
+
+    def sweep(self, direction: int, dt: float):
+        _check(_lib.how_sweep(self._h, direction, dt))
+
+    def run(self, time=0.0, max_steps=-1, dts_cap=0):
+        t = ctypes.c_double(time)
+        s = ctypes.c_long(0)
+        dts = np.zeros(max(dts_cap, 1))
+        _check(_lib.how_run(self._h, ctypes.byref(t), max_steps, ctypes.byref(s), _dptr(dts), dts_cap))
+        return t.value, s.value, dts[: min(s.value, dts_cap)].copy()
+
+    def set_precision(self, mode):
+        if isinstance(mode, str):
+            mode = {"fp64": HOW_PREC_FP64, "mixed": HOW_PREC_MIXED}[mode]
+        _check(_lib.how_set_precision(self._h, mode))
+
+    def sync(self):
+        _check(_lib.how_sync(self._h))
+
+    @property
+    def kernel_launches(self) -> int:
+        return _lib.how_kernel_launches(self._h)
+
+    @property
+    def stream(self) -> int:
+        return _lib.how_stream(self._h) or 0
+
+    @property
+    def device_bytes(self) -> int:
+        return _lib.how_device_bytes(self._h)
+
+
+# reference-named free functions over a Domain
+def init_problem(dom: Domain):
+    """init_problem + bound(q,0) + initialize_bfield_from_q (src/main.cpp:125-130)."""
+    dom.init_problem()
+
+
+def bound(dom: Domain, stage: int):
+    dom.bound(stage)
+
+
+def bound_bfield(dom: Domain, stage: int):
+    dom.bound_bfield(stage)
+
+
+def tstep(dom: Domain) -> float:
+    return dom.tstep()
+
+
+def ssprk(dom: Domain, dt: float):
+    dom.ssprk(dt)
+
+
+def prot(dom: Domain, stage: int):
+    dom.prot(stage)

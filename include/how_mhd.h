@@ -1,0 +1,171 @@
+/* how_mhd.h -- C ABI of the B200-native HOW-MHD time-step path.
+ *
+ * Drop-in for the reference's driver-level surface (jeongbhin/HOW-MHD-Kokkos,
+ * paths inside that project).  Every entry point names the reference function
+ * it replaces.  All calls return HOW_OK (0) or a negative HOW_ERR_* code; the
+ * message of the last failure on the calling thread is how_last_error().
+ * Nothing aborts the process.
+ *
+ * State layout at the boundary is the reference's: one stage of q is
+ * 8 variables (rho, mx, my, mz, Bx, By, Bz, E) x (nx+6) x (ny+6) x (nz+6)
+ * doubles with k fastest (LayoutRight of q(stage, var, i, j, k),
+ * src/main.cpp:101-120); active cells are i,j,k in [3, n+2].  A face-B
+ * component is (nx+6)x(ny+6)x(nz+6) doubles, bxb(i) being the x-face at i+1/2
+ * (src/fluxct.cpp:27-35, 84-88).  The device keeps its own x-fastest layout;
+ * conversion happens only on upload/download.
+ *
+ * All device work of a context is ordered on the context's CUDA stream.
+ * Calls on one context are not thread-safe.  Device-side faults are reported
+ * through status words (HOW_ERR_NONFINITE, ...), never by trapping.
+ */
+#ifndef HOW_MHD_H
+#define HOW_MHD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HOW_OK 0
+#define HOW_ERR_ARG (-1)        /* invalid argument or size                  */
+#define HOW_ERR_PARSE (-2)      /* input.in value missing or invalid          */
+#define HOW_ERR_PROBLEM (-3)    /* unknown problem name                       */
+#define HOW_ERR_CUDA (-4)       /* CUDA runtime error (message has details)   */
+#define HOW_ERR_NODEVICE (-5)   /* no CUDA device / extension not usable      */
+#define HOW_ERR_NONFINITE (-6)  /* time or dt became non-finite               */
+#define HOW_ERR_DT (-7)         /* non-positive dt (src/main.cpp:175-183)     */
+#define HOW_ERR_STATE (-8)      /* call out of order (e.g. no state yet)      */
+
+#define HOW_BC_PERIODIC 0
+#define HOW_BC_OPEN 1
+
+#define HOW_PREC_FP64 0         /* plain FP64 method (the reference's)        */
+#define HOW_PREC_MIXED 1        /* FP32 eigen/projection/WENO, FP64 RK/CT/CFL */
+
+/* Parameters: struct Parameters (src/parameters.hpp:10-76).  nx/ny/nz are the
+ * global active-cell counts (the reference's gnx/gny/gnz; one device-resident
+ * domain, so local == global).  px/py/pz are parsed and ignored, like the
+ * reference's serial build (src/mpi_domain.cpp:87-90). */
+typedef struct how_params {
+    int nx, ny, nz;
+    int nt, nstep, ntime;
+    double xsize, ysize, zsize;
+    double dx, dy, dz;
+    double gam, cour, tend, rhomin, pgmin;
+    int bc[3];                 /* x1bc, x2bc, x3bc */
+    int px, py, pz;
+    char problem[64];
+    char output_format[16];
+    /* keys added by this implementation; the reference parser warns on them
+     * and skips the line (src/parameters.cpp:112-116), so input files that
+     * use them stay readable by the reference. */
+    int precision;             /* HOW_PREC_*                      (key: precision fp64|mixed) */
+    int router;                /* 0 off, 1 learned WENO routing   (key: router off|on)        */
+    uint64_t seed;             /* problem seed                    (key: seed)                 */
+    double problem_par[8];     /* problem parameters              (keys: par0..par7)          */
+} how_params;
+
+typedef struct how_ctx how_ctx;
+
+/* Problem initialiser: fill stage 0 of q (reference layout, ghosts may be
+ * left untouched) from the parameters.  Returns 0 on success. */
+typedef int (*how_problem_fn)(double* q, const how_params* par, void* user);
+
+/* ------------------------------------------------------------ parameters */
+/* read_parameters + finalize_parameters_after_read
+ * (src/parameters.cpp:7-118, 120-160): defaults, whitespace key/value pairs,
+ * '#' comments to end of line, unknown keys warned to stderr and skipped;
+ * validation (positive sizes, nt > 0, tend > 0) returns HOW_ERR_PARSE
+ * instead of aborting.  dx = size / n. */
+int how_params_default(how_params* p);
+int how_parse_input(const char* path, how_params* p);
+int how_parse_input_string(const char* text, how_params* p);
+int how_finalize_params(how_params* p);
+
+/* --------------------------------------------------------------- problems */
+/* register_problem / RegisterProblem (src/problem.hpp:8-22).  Built-in
+ * names: orszag_tang, blast3d, brio_wu, mhd_rotor, uniform, mpi_smooth3d
+ * (the reference's), plus alfven3d, blast3d_b, turb3d (new). */
+int how_register_problem(const char* name, how_problem_fn fn, void* user);
+/* newline-separated registered names into buf; returns the count */
+int how_list_problems(char* buf, size_t cap);
+/* init_problem (src/problem.cpp:17-37) on the host, no device needed:
+ * fills q_host (one stage, reference layout) from the registry. */
+int how_problem_init_host(const how_params* p, double* q_host);
+
+/* ---------------------------------------------------------------- context */
+/* Allocates q(6 stages), face B(6 stages) and the CT arrays on the current
+ * CUDA device (the reference allocates in main.cpp:114-120 and
+ * allocate_bfield_ct, src/fluxct.cpp:27-35). */
+int how_create(const how_params* p, how_ctx** out);
+int how_destroy(how_ctx* ctx);
+const char* how_last_error(void);
+int how_get_params(const how_ctx* ctx, how_params* out);
+/* Bytes of device memory the context holds. */
+size_t how_device_bytes(const how_ctx* ctx);
+
+/* init_problem + bound(q,0) + initialize_bfield_from_q (src/main.cpp:125-130) */
+int how_init_problem(how_ctx* ctx);
+
+/* ------------------------------------------------------------------ state */
+/* Upload / download one stage (reference layout, host memory).  Pinned host
+ * buffers make the copies asynchronous-capable; pageable also works. */
+int how_set_state(how_ctx* ctx, int stage, const double* q_host);
+int how_get_state(how_ctx* ctx, int stage, double* q_host);
+int how_set_face_b(how_ctx* ctx, int stage, const double* bx, const double* by, const double* bz);
+int how_get_face_b(how_ctx* ctx, int stage, double* bx, double* by, double* bz);
+
+/* -------------------------------------------------------- path functions */
+/* bound (src/bound.cpp:295-317): periodic/open ghost fill x, then y, then z */
+int how_bound(how_ctx* ctx, int stage);
+/* bound_bfield (src/fluxct.cpp:481-490) */
+int how_bound_bfield(how_ctx* ctx, int stage);
+/* initialize_bfield_from_q (src/fluxct.cpp:65-107): needs bound(q,0) first */
+int how_init_bfield_from_q(how_ctx* ctx);
+/* tstep (src/tstep.cpp:11-136): CFL dt from stage 0; returns it in *dt */
+int how_tstep(how_ctx* ctx, double* dt);
+/* ssprk (src/ssprk.cpp:1277-1329): one SSPRK(5,4) step with the given dt, in
+ * place on stage 0 (q and face B). */
+int how_ssprk(how_ctx* ctx, double dt);
+/* prot (src/prot.cpp:6-54) on one stage */
+int how_prot(how_ctx* ctx, int stage);
+/* One directional sweep of stage 1 (src/ssprk.cpp:1000-1025, 1218-1272)
+ * exactly as the reference's x_sweep/y_sweep/z_sweep would run it inside
+ * stage 1 of ssprk with this dt: copies q(0) to q(1) first.  dir 0,1,2. */
+int how_sweep(how_ctx* ctx, int dir, double dt);
+/* Download a CT flux array (0..5 = fsy fsz gsx gsz hsx hsy) in the reference
+ * layout, for inspection after how_sweep / how_ssprk. */
+int how_get_ct_array(how_ctx* ctx, int which, double* host);
+
+/* Main loop (src/main.cpp:158-223) without output: advances from *time for
+ * up to max_steps steps (max_steps < 0: no limit) towards tend, with the
+ * reference's nt output intervals and dt clamp to each interval's end.
+ * Updates *time and *steps.  dts (may be NULL) receives each step's dt. */
+int how_run(how_ctx* ctx, double* time, long max_steps, long* steps, double* dts, long dts_cap);
+
+/* How the sweeps compute (HOW_PREC_*). */
+int how_set_precision(how_ctx* ctx, int mode);
+
+/* Block until the context's stream is idle. */
+int how_sync(how_ctx* ctx);
+
+/* ------------------------------------------------------ instrumentation */
+/* Launches of this library's kernels since the context was created. */
+long how_kernel_launches(const how_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for callers that time with events. */
+void* how_stream(how_ctx* ctx);
+/* CUDA-event timing of every sweep-kernel launch while enabled (no reference
+ * counterpart; the reference has no timers).  Enabling clears the record. */
+int how_set_kernel_timing(how_ctx* ctx, int on);
+/* Summed device milliseconds and count of the timed sweep launches. */
+int how_get_kernel_timing(how_ctx* ctx, double* total_ms, long* launches);
+/* Measured FP64 FMA-pipe throughput of the current device, TFLOP/s (2 flops
+ * per FMA): the roofline denominator of this FP64-bound path. */
+int how_measure_fp64_peak(double* tflops, int reps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HOW_MHD_H */

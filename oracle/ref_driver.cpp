@@ -177,7 +177,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     std::string input = argv[1], out = argv[2];
-    long max_steps = -1;
+    long max_steps = -1, warmup = 0;
     std::string state_path, sweep;
     double sweep_dt = 0.0;
     bool dump_stages = false, time_only = false;
@@ -190,6 +190,7 @@ int main(int argc, char** argv) {
         else if (s == "--dt" && a + 1 < argc) sweep_dt = std::atof(argv[++a]);
         else if (s == "--threads" && a + 1 < argc) omp_set_num_threads(std::atoi(argv[++a]));
         else if (s == "--time-only") time_only = true;
+        else if (s == "--warmup" && a + 1 < argc) warmup = std::atol(argv[++a]);
         else { std::fprintf(stderr, "unknown option %s\n", s.c_str()); return 2; }
     }
 
@@ -274,11 +275,14 @@ int main(int argc, char** argv) {
             std::vector<double> dts;
             long steps = 0;
             bool stop = false;
+            // --warmup W: W untimed steps first (same loop), then K timed
             double t0 = omp_get_wtime();
+            long timed_from = 0;
             for (int out_step = 1; out_step <= par.nt && !stop; ++out_step) {
                 const double target_time = dtout * static_cast<double>(out_step);
                 while (time < target_time) {
-                    if (max_steps >= 0 && steps >= max_steps) { stop = true; break; }
+                    if (max_steps >= 0 && steps >= max_steps + warmup) { stop = true; break; }
+                    if (steps == warmup && timed_from == 0) { t0 = omp_get_wtime(); timed_from = steps; }
                     tstep(q, par);
                     if (time + par.dt > target_time) par.dt = target_time - time;
                     if (par.dt <= 0.0) { rc = 3; stop = true; break; }
@@ -290,11 +294,12 @@ int main(int argc, char** argv) {
                 }
             }
             double wall = omp_get_wtime() - t0;
+            const long timed = steps - timed_from;
             if (time_only) {
                 const double zones = (double)par.nx * par.ny * par.nz;
-                std::printf("{\"steps\": %ld, \"wall_s\": %.6f, \"zone_cycles_per_s\": %.6e, "
+                std::printf("{\"steps\": %ld, \"warmup\": %ld, \"wall_s\": %.6f, \"zone_cycles_per_s\": %.6e, "
                             "\"threads\": %d, \"time\": %.17g}\n",
-                            steps, wall, steps > 0 ? zones * steps / wall : 0.0,
+                            timed, warmup, wall, timed > 0 ? zones * timed / wall : 0.0,
                             omp_get_max_threads(), time);
             } else {
                 Writer w(out);
