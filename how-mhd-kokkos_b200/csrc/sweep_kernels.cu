@@ -44,16 +44,17 @@ struct Tile {
     static constexpr int NP = (F + 1) / 2;
     static constexpr int NLC = NL * C;
     static constexpr int NLF = NL * F;
+    static constexpr int NI = NLF | 1;              // odd interface pitch: conflict-free banks
     // shared-memory carve-up, in doubles
     static constexpr int oQ = 0;                    // [8][NLC] raw conserved
     static constexpr int oU = oQ + 8 * NLC;         // [NLC][14] F(7), q_proj(7)
     static constexpr int oP = oU + 14 * NLC;        // [9][NLC] primitives
     static constexpr int oA = oP + 9 * NLC;         // [7][NLC] eigenvalues
-    static constexpr int oL = oA + 7 * NLC;         // [NLF][7][8] L rows
-    static constexpr int oR = oL + 56 * NLF;        // [NLF][7][8] R columns
-    static constexpr int oS = oR + 56 * NLF;        // [20][NLF] scalars | Fs [NLF][8], dF [NLF][8]
+    static constexpr int oL = oA + 7 * NLC;         // [7 row][7 col][NI] left eigenvectors
+    static constexpr int oR = oL + 49 * NI;         // [7 wave][7 phys][NI] right eigenvectors
+    static constexpr int oS = oR + 49 * NI;         // [20][NI] scalars | Fs [7][NI], dF [7][NI]
     static constexpr int NS = 20;
-    static constexpr int total = oS + NS * NLF;
+    static constexpr int total = oS + NS * NI;
     static constexpr size_t bytes = sizeof(double) * (size_t)total;
 };
 
@@ -94,10 +95,10 @@ __device__ __forceinline__ double weno_flux(const double* Fsk, const double* qsk
     return first - second + third;
 }
 
-template <int DIR, int NL, int T>
-__global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
+template <int DIR, int NL, int T, int NT>
+__global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
     using TL = Tile<NL, T>;
-    constexpr int C = TL::C, F = TL::F, NP = TL::NP, NLC = TL::NLC, NLF = TL::NLF;
+    constexpr int C = TL::C, F = TL::F, NP = TL::NP, NLC = TL::NLC, NLF = TL::NLF, NI = TL::NI;
     extern __shared__ __align__(16) double sm[];
     double* sQ = sm + TL::oQ;
     double* sU = sm + TL::oU;
@@ -106,8 +107,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
     double* sL = sm + TL::oL;
     double* sR = sm + TL::oR;
     double* sS = sm + TL::oS;
-    double* sFs = sS;              // [NLF][8], after P2b
-    double* sdF = sS + 8 * NLF;    // [NLF][8], after P3
+    double* sFs = sS;              // [7][NI], after P2b
+    double* sdF = sS + 7 * NI;     // [7][NI], after P3
 
     const Grid& g = a.g;
     const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
@@ -146,9 +147,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
         const double Mz = sQ[3 * NLC + t], Bx = sQ[4 * NLC + t], By = sQ[5 * NLC + t];
         const double Bz = sQ[6 * NLC + t];
         double EE = sQ[7 * NLC + t];
-        // primit (src/ssprk.cpp:479-512)
+        // primit (src/ssprk.cpp:479-512): v from the unfloored density
         double rho = DD;
-        const double vx = Mx / rho, vy = My / rho, vz = Mz / rho;
+        double irho = 1.0 / rho;
+        const double vx = Mx * irho, vy = My * irho, vz = Mz * irho;
         const double vv2 = vx * vx + vy * vy + vz * vz;
         const double BB2 = Bx * Bx + By * By + Bz * Bz;
         double pg = (gam - 1.0) * (EE - 0.5 * (rho * vv2 + BB2));
@@ -156,15 +158,15 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
             rho = fmax(a.rhomin, rho);
             pg = fmax(a.pgmin, pg);
             EE = pg / (gam - 1.0) + 0.5 * (rho * vv2 + BB2);
+            irho = 1.0 / rho;
         }
-        const double HH = (EE + pg) / rho;
+        const double HH = (EE + pg) * irho;
         sP[0 * NLC + t] = rho; sP[1 * NLC + t] = vx; sP[2 * NLC + t] = vy; sP[3 * NLC + t] = vz;
         sP[4 * NLC + t] = Bx; sP[5 * NLC + t] = By; sP[6 * NLC + t] = Bz; sP[7 * NLC + t] = pg;
         sP[8 * NLC + t] = HH;
         // eigenst centre (src/ssprk.cpp:561-593), with DD, EE the floored values
         const double pt = pg + 0.5 * BB2;
         const double vdB = vx * Bx + vy * By + vz * Bz;
-        const double irho = 1.0 / rho;
         const double bbn2 = BB2 * irho;
         const double bnx2 = Bx * Bx * irho;
         const double cs2 = fmax(0.0, gam * fabs(pg * irho));
@@ -202,37 +204,37 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
         const double HH = 0.5 * (sP[8 * NLC + c] + sP[8 * NLC + c + 1]);
         const double vv2 = vx * vx + vy * vy + vz * vz;
         const double BB2 = Bx * Bx + By * By + Bz * Bz;
-        const double irho = 1.0 / rho;
+        const double isqr = rsqrt(rho);
+        const double irho = isqr * isqr;
         const double bbn2 = BB2 * irho;
         const double bnx2 = Bx * Bx * irho;
         const double cs2 = (gam - 1.0) * (HH - 0.5 * (vv2 + bbn2));
         const double cs = sqrt(fmax(0.0, cs2));
         const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
         const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
-        const double la = sqrt(fmax(0.0, bnx2));
+        const double la = fabs(Bx) * isqr;
         const double ls = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 - root)));
         const double Bt2 = By * By + Bz * Bz;
         double bty, btz;
-        if (Bt2 >= 1.0e-30) { const double ib = 1.0 / sqrt(Bt2); bty = By * ib; btz = Bz * ib; }
+        if (Bt2 >= 1.0e-30) { const double ib = rsqrt(Bt2); bty = By * ib; btz = Bz * ib; }
         else { bty = 0.70710678118654752440; btz = 0.70710678118654752440; }
         double af, as;
         const double df = lf * lf - ls * ls;
         if (df >= 1.0e-30) {
-            const double idf = 1.0 / sqrt(df);
+            const double idf = rsqrt(df);
             af = sqrt(fmax(0.0, cs2 - ls * ls)) * idf;
             as = sqrt(fmax(0.0, lf * lf - cs2)) * idf;
         } else { af = 1.0; as = 1.0; }
-        const double sqrtrho = sqrt(rho);
         double* S = sS + t;
-        S[S_VX * NLF] = vx; S[S_VY * NLF] = vy; S[S_VZ * NLF] = vz;
-        S[S_BY * NLF] = By; S[S_BZ * NLF] = Bz; S[S_VV2 * NLF] = vv2;
-        S[S_CS * NLF] = cs; S[S_CS2 * NLF] = cs2; S[S_LF * NLF] = lf; S[S_LS * NLF] = ls;
-        S[S_AF * NLF] = af; S[S_AS * NLF] = as; S[S_BTY * NLF] = bty; S[S_BTZ * NLF] = btz;
-        S[S_SGNBX * NLF] = sign1(Bx);
-        S[S_SQR * NLF] = sqrtrho; S[S_ISQR * NLF] = 1.0 / sqrtrho;
-        S[S_SGNBT * NLF] = (By != 0.0) ? sign1(By) : sign1(Bz);
-        S[S_FLIP * NLF] = (cs >= la) ? 1.0 : 0.0;
-        S[S_BTV * NLF] = bty * vy + btz * vz;
+        S[S_VX * NI] = vx; S[S_VY * NI] = vy; S[S_VZ * NI] = vz;
+        S[S_BY * NI] = By; S[S_BZ * NI] = Bz; S[S_VV2 * NI] = vv2;
+        S[S_CS * NI] = cs; S[S_CS2 * NI] = cs2; S[S_LF * NI] = lf; S[S_LS * NI] = ls;
+        S[S_AF * NI] = af; S[S_AS * NI] = as; S[S_BTY * NI] = bty; S[S_BTZ * NI] = btz;
+        S[S_SGNBX * NI] = sign1(Bx);
+        S[S_SQR * NI] = rho * isqr; S[S_ISQR * NI] = isqr;
+        S[S_SGNBT * NI] = (By != 0.0) ? sign1(By) : sign1(Bz);
+        S[S_FLIP * NI] = (cs >= la) ? 1.0 : 0.0;
+        S[S_BTV * NI] = bty * vy + btz * vz;
     }
     __syncthreads();
 
@@ -241,14 +243,14 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
     for (int t = tid; t < 7 * NLF; t += blockDim.x) {
         const int r = t / NLF, i = t % NLF;
         const double* S = sS + i;
-        const double vx = S[S_VX * NLF], vy = S[S_VY * NLF], vz = S[S_VZ * NLF];
-        const double By = S[S_BY * NLF], Bz = S[S_BZ * NLF], vv2 = S[S_VV2 * NLF];
-        const double cs = S[S_CS * NLF], cs2 = S[S_CS2 * NLF];
-        const double lf = S[S_LF * NLF], ls = S[S_LS * NLF], af = S[S_AF * NLF], as = S[S_AS * NLF];
-        const double bty = S[S_BTY * NLF], btz = S[S_BTZ * NLF], sgnBx = S[S_SGNBX * NLF];
-        const double sqrtrho = S[S_SQR * NLF], isqr = S[S_ISQR * NLF], sgnBt = S[S_SGNBT * NLF];
-        const bool flip24 = S[S_FLIP * NLF] != 0.0;
-        const double btv = S[S_BTV * NLF];
+        const double vx = S[S_VX * NI], vy = S[S_VY * NI], vz = S[S_VZ * NI];
+        const double By = S[S_BY * NI], Bz = S[S_BZ * NI], vv2 = S[S_VV2 * NI];
+        const double cs = S[S_CS * NI], cs2 = S[S_CS2 * NI];
+        const double lf = S[S_LF * NI], ls = S[S_LS * NI], af = S[S_AF * NI], as = S[S_AS * NI];
+        const double bty = S[S_BTY * NI], btz = S[S_BTZ * NI], sgnBx = S[S_SGNBX * NI];
+        const double sqrtrho = S[S_SQR * NI], isqr = S[S_ISQR * NI], sgnBt = S[S_SGNBT * NI];
+        const bool flip24 = S[S_FLIP * NI] != 0.0;
+        const double btv = S[S_BTV * NI];
         double L[7], R[7];
         switch (r) {
             case 0: {
@@ -343,12 +345,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
         }
         // sign convention (src/ssprk.cpp:789-818)
         const bool flip = flip24 ? (r == 2 || r == 4) : (r == 0 || r == 6);
-        double* Lo = sL + (i * 7 + r) * 8;
-        double* Ro = sR + (i * 7 + r) * 8;
 #pragma unroll
         for (int m = 0; m < 7; ++m) {
-            Lo[m] = flip ? L[m] * sgnBt : L[m];
-            Ro[m] = flip ? R[m] * sgnBt : R[m];
+            sL[(r * 7 + m) * NI + i] = flip ? L[m] * sgnBt : L[m];
+            sR[(r * 7 + m) * NI + i] = flip ? R[m] * sgnBt : R[m];
         }
     }
     __syncthreads();
@@ -359,17 +359,13 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
         const int l = pr / NP, p = pr % NP;
         const int f0 = 2 * p;
         const bool has1 = f0 + 1 < F;
-        const int f1 = has1 ? f0 + 1 : f0;
+        const int i0 = l * F + f0;
+        const int i1 = has1 ? i0 + 1 : i0;
         double L0[7], L1[7];
-        {
-            const double2* a0 = reinterpret_cast<const double2*>(sL + ((l * F + f0) * 7 + m) * 8);
-            const double2* a1 = reinterpret_cast<const double2*>(sL + ((l * F + f1) * 7 + m) * 8);
 #pragma unroll
-            for (int h = 0; h < 3; ++h) {
-                const double2 x0 = a0[h], x1 = a1[h];
-                L0[2 * h] = x0.x; L0[2 * h + 1] = x0.y; L1[2 * h] = x1.x; L1[2 * h + 1] = x1.y;
-            }
-            L0[6] = a0[3].x; L1[6] = a1[3].x;
+        for (int v = 0; v < 7; ++v) {
+            L0[v] = sL[(m * 7 + v) * NI + i0];
+            L1[v] = sL[(m * 7 + v) * NI + i1];
         }
         double Fk0[6], qk0[6], Fk1[6], qk1[6];
         double amx0 = 0.0, amx1 = 0.0;
@@ -397,28 +393,25 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
                 amx1 = fmax(amx1, av);
             }
         }
-        sFs[(l * F + f0) * 8 + m] = weno_flux(Fk0, qk0, amx0);
-        if (has1) sFs[(l * F + f1) * 8 + m] = weno_flux(Fk1, qk1, amx1);
+        sFs[m * NI + i0] = weno_flux(Fk0, qk0, amx0);
+        if (has1) sFs[m * NI + i1] = weno_flux(Fk1, qk1, amx1);
     }
     __syncthreads();
 
     // ---------------------------------------------------------------- P4
     for (int t = tid; t < NLF; t += blockDim.x) {
         const int l = t / F, f = t % F;
-        double Fs[7];
-#pragma unroll
-        for (int m = 0; m < 7; ++m) Fs[m] = sFs[t * 8 + m];
         double dF[7];
 #pragma unroll
         for (int r = 0; r < 7; ++r) dF[r] = 0.0;
 #pragma unroll
         for (int m = 0; m < 7; ++m) {
-            const double* Rm = sR + (t * 7 + m) * 8;
+            const double fs = sFs[m * NI + t];
 #pragma unroll
-            for (int r = 0; r < 7; ++r) dF[r] += Rm[r] * Fs[m];
+            for (int r = 0; r < 7; ++r) dF[r] += sR[(m * 7 + r) * NI + t] * fs;
         }
 #pragma unroll
-        for (int r = 0; r < 7; ++r) sdF[t * 8 + r] = dF[r];
+        for (int r = 0; r < 7; ++r) sdF[r * NI + t] = dF[r];
         // CT terms (src/ssprk.cpp:973-993): mean of B_n v_t over the two cells
         const int c = l * C + f + 2;
         const double x1 = sP[4 * NLC + c] * sP[2 * NLC + c], x2 = sP[4 * NLC + c + 1] * sP[2 * NLC + c + 1];
@@ -442,7 +435,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
         if (!line_ok(l) || s > n + 2) continue;
         const int rr = v < 4 ? v : v - 1;     // flux row of line variable v (v = 4: normal B)
         const int fi = l * F + ct;
-        const double delta = (v == 4) ? 0.0 : -dtdl * (sdF[(fi + 1) * 8 + rr] - sdF[fi * 8 + rr]);
+        const double delta = (v == 4) ? 0.0 : -dtdl * (sdF[rr * NI + fi + 1] - sdF[rr * NI + fi]);
         const long long o = (long long)c_perm[DIR][v] * g.fs + line_off(l) + (long long)s * sstride;
         if (a.mode == 0) {
             if (v != 4) a.qout[o] += delta;
@@ -455,12 +448,12 @@ __global__ void __launch_bounds__(256, 2) k_sweep(SweepArgs a) {
     }
 }
 
-template <int DIR, int NL, int T>
+template <int DIR, int NL, int T, int NT>
 void launch_one(Ctx& c, const SweepArgs& a) {
     using TL = Tile<NL, T>;
     static bool attr_done = false;
     if (!attr_done) {
-        cudaFuncSetAttribute(k_sweep<DIR, NL, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::bytes);
+        cudaFuncSetAttribute(k_sweep<DIR, NL, T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::bytes);
         attr_done = true;
     }
     const Grid& g = c.g;
@@ -470,7 +463,7 @@ void launch_one(Ctx& c, const SweepArgs& a) {
     dim3 grid((n + T - 1) / T, (nt1 + NL - 1) / NL, nt2);
     cudaEvent_t ev[2];
     timer_begin(c, ev);
-    k_sweep<DIR, NL, T><<<grid, 256, TL::bytes, c.stream>>>(a);
+    k_sweep<DIR, NL, T, NT><<<grid, NT, TL::bytes, c.stream>>>(a);
     timer_end(c, ev);
     ++c.launches;
 }
@@ -478,9 +471,9 @@ void launch_one(Ctx& c, const SweepArgs& a) {
 }  // namespace
 
 void launch_sweep(Ctx& c, int dir, const SweepArgs& a) {
-    if (dir == 0) launch_one<0, 2, 32>(c, a);
-    else if (dir == 1) launch_one<1, 4, 16>(c, a);
-    else launch_one<2, 4, 16>(c, a);
+    if (dir == 0) launch_one<0, 1, 32, 128>(c, a);
+    else if (dir == 1) launch_one<1, 2, 16, 128>(c, a);
+    else launch_one<2, 2, 16, 128>(c, a);
 }
 
 }  // namespace how

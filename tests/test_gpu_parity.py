@@ -12,7 +12,11 @@ from howtest import CPUOracle, active, rel_l1
 pytestmark = pytest.mark.gpu
 
 TOL_Q = 1e-12
-TOL_DT = 1e-14
+# dt of the fast FP64 path: the reference's own dt moves by up to 4.7e-14
+# (Orszag-Tang, 10 steps) when its initial state is perturbed by 1e-16, so a
+# path that rounds differently cannot be held to 1e-14; 1e-13 is ~2x that
+# self-sensitivity.  The bit-reproducing mode is held to 0.
+TOL_DT = 1e-13
 
 
 def _hm():
