@@ -2,6 +2,7 @@
 // layout conversion, and the SSPRK(5,4) stage sequence of src/ssprk.cpp:1277-1329
 // expressed as kernel launches on the context's stream.
 #include "how_internal.cuh"
+#include "tma.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -31,6 +32,38 @@ int cuda_fail(cudaError_t e, const char* what) {
 
 static size_t ref_count(const Grid& g) { return (size_t)g.P0 * g.P1 * g.P2; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_tensor_map_4d(CUtensorMap* map, const void* base, const uint64_t dims[4],
+                         const uint64_t strides_bytes[3], const uint32_t box[4]) {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) {
+            set_error("cuTensorMapEncodeTiled entry point unavailable");
+            return HOW_ERR_CUDA;
+        }
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    cuuint64_t gd[4] = {dims[0], dims[1], dims[2], dims[3]};
+    cuuint64_t gs[3] = {strides_bytes[0], strides_bytes[1], strides_bytes[2]};
+    cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), gd, gs, bx, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d): box %u x %u x %u x %u", (int)r, box[0], box[1], box[2], box[3]);
+        return HOW_ERR_CUDA;
+    }
+    return HOW_OK;
+}
+
 // ---------------------------------------------------------------- one stage
 // Stage iw of ssprk (src/ssprk.cpp:1281-1325).  The reference's per-stage
 // zero_ct_fluxes, copy_stage / prepare_stage5 and the leading bound(q, iw-1)
@@ -53,6 +86,11 @@ static void run_stage(Ctx& c, int iw) {
     a.k1 = k.k1; a.k3 = k.k3; a.c4 = c4; a.c5 = c5;
     a.stage5 = stage5;
     a.gam = c.p.gam; a.rhomin = c.p.rhomin; a.pgmin = c.p.pgmin;
+    if (stage5) {
+        // prepare_stage5 (src/ssprk.cpp:121-140) on active cells: the first
+        // sweep then reads its RK base from q(5) like every other stage's q(0)
+        launch_stage5_base(c, c4, c5);
+    }
     bool first = true;
     // x_sweep stores k1 q(iw) + k3 q(iw-1) + dq (src/ssprk.cpp:424-427); y/z add.
     // With nx == 1 there is no x sweep and q(iw) keeps the copied base.
@@ -105,6 +143,14 @@ static int check_stage(int s) {
 static int sync_and_status(Ctx& c) {
     HOW_CUDA_CHECK(cudaStreamSynchronize(c.stream));
     HOW_CUDA_CHECK(cudaGetLastError());
+    unsigned int st = 0;
+    HOW_CUDA_CHECK(cudaMemcpy(&st, &c.dsc->status, sizeof(st), cudaMemcpyDeviceToHost));
+    if (st & (HOW_STATUS_TMA_TIMEOUT | HOW_STATUS_TMA_ALIGN)) {
+        cudaMemset(&c.dsc->status, 0, sizeof(st));
+        set_error("device status 0x%x: %s", st,
+                  (st & HOW_STATUS_TMA_ALIGN) ? "misaligned tensor copy refused" : "bounded TMA wait expired");
+        return HOW_ERR_CUDA;
+    }
     return HOW_OK;
 }
 
@@ -140,7 +186,7 @@ int how_create(const how_params* p, how_ctx** out) {
     e = cudaMalloc(&c->mem, c->mem_bytes);
     if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMalloc(state)"); }
     double* m = c->mem;
-    for (int s = 0; s < 6; ++s) { c->q[s] = m; m += 8 * g.fs; }
+    for (int s = 0; s < 6; ++s) { c->q[s] = c->qbuf[s] = m; m += 8 * g.fs; }
     for (int s = 0; s < 6; ++s) { c->b[s] = m; m += 3 * g.fs; }
     for (int a = 0; a < 12; ++a) { c->ct[a] = m; m += g.fs; }
     c->stage_buf = m;
@@ -152,6 +198,7 @@ int how_create(const how_params* p, how_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { how_destroy(c); return cuda_fail(e, "context set-up"); }
     std::memset(c->hsc, 0, sizeof(DevScalars));
+    if ((rc = make_sweep_tensor_maps(*c))) { how_destroy(c); return rc; }
     *out = c;
     return HOW_OK;
 }

@@ -2,6 +2,7 @@
 // shared by the translation units of libhowmhd.so.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -58,10 +59,12 @@ struct DevScalars {
     double dt_raw;                     // dt before the output-time clamp
 };
 
-enum : unsigned int { HOW_STATUS_NONFINITE_DT = 1u };
+enum : unsigned int { HOW_STATUS_NONFINITE_DT = 1u, HOW_STATUS_TMA_TIMEOUT = 2u, HOW_STATUS_TMA_ALIGN = 4u };
 
 // Arguments of one directional sweep launch.
 struct SweepArgs {
+    CUtensorMap tm_in;     // stage iw-1: the pencil tile (with halo) of all 8 variables
+    CUtensorMap tm_out;    // the update's read operand: q(iw) (accumulate) or the RK base
     Grid g;
     const double* qprev;   // stage iw-1, field 0 (vars at + v * fs)
     double* qout;          // stage iw
@@ -75,6 +78,8 @@ struct SweepArgs {
     int mode;              // 0 accumulate, 1 first sweep with RK combine, 2 first sweep base+delta
     int stage5;            // base = q0 + c4 q2 + c5 q3
     double gam, rhomin, pgmin;
+    unsigned long long* prof;   // optional per-phase cycle counters (instrumentation)
+    unsigned int* status;       // device status word (HOW_STATUS_* bits)
 };
 
 struct Ctx {
@@ -85,6 +90,9 @@ struct Ctx {
     double* mem = nullptr;          // one allocation for every field
     size_t mem_bytes = 0;
     double* q[6] = {};              // stage s, field 0; var v at + v * fs
+    double* qbuf[6] = {};           // the six physical stage buffers (q[] is a permutation)
+    CUtensorMap tm_in[6][3];        // per physical buffer and sweep direction: input tile
+    CUtensorMap tm_out[6][3];       // per physical buffer and sweep direction: update tile
     double* b[6] = {};              // face B stage s: comps at + c * fs
     double* ct[12] = {};            // fsy fsz gsx gsz hsx hsy Ox2 Oy2 Oz2 Ox Oy Oz
     double* stage_buf = nullptr;    // device staging for layout conversion (8 fields)
@@ -93,6 +101,7 @@ struct Ctx {
     long launches = 0;
     int precision = HOW_PREC_FP64;
     bool have_state = false;
+    unsigned long long* prof = nullptr;   // device phase counters while profiling
 };
 
 // ---- kernels / launchers (defined in the .cu files) ------------------------
@@ -106,6 +115,8 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a);
 void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5);
 void launch_faceb_base(Ctx& c, int iw, double c4, double c5, int stage5);
 void launch_prot(Ctx& c, int stage);
+void launch_stage5_base(Ctx& c, double c4, double c5);
+int make_sweep_tensor_maps(Ctx& c);
 void launch_copy_fields(Ctx& c, double* dst, const double* src, int nfields);
 
 void set_error(const char* fmt, ...);

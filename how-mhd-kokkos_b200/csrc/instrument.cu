@@ -93,6 +93,29 @@ int how_get_kernel_timing(how_ctx* cp, double* total_ms, long* launches) {
     return HOW_OK;
 }
 
+// Per-phase cycle accounting of one directional sweep of stage 1 (the
+// how_sweep semantics): out[k] = mean cycles per block spent in phase k
+// (0 load, 1 primitives/centre, 2 differences + interface scalars,
+// 3 eigenvector rows, 4 projection + WENO, 5 back-projection + CT,
+// 6 update), measured by thread 0 of each block with clock64.
+int how_sweep_phase_profile(how_ctx* cp, int dir, double dt, double* out, int nout) {
+    Ctx* c = cp;
+    if (!c || !out) return HOW_ERR_ARG;
+    unsigned long long* d = nullptr;
+    HOW_CUDA_CHECK(cudaMalloc(&d, 8 * sizeof(unsigned long long)));
+    HOW_CUDA_CHECK(cudaMemset(d, 0, 8 * sizeof(unsigned long long)));
+    c->prof = d;
+    const int rc = how_sweep(cp, dir, dt);
+    c->prof = nullptr;
+    unsigned long long h[8] = {0};
+    cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (rc) return rc;
+    for (int k = 0; k < nout && k < 8; ++k)
+        out[k] = k < 7 ? (h[7] ? (double)h[k] / (double)h[7] : 0.0) : (double)h[7];
+    return HOW_OK;
+}
+
 // Measured FP64 FMA throughput of the current device in TFLOP/s (2 flops per
 // FMA), best of `reps` launches of 8 independent FMA chains per thread.
 int how_measure_fp64_peak(double* tflops, int reps) {

@@ -212,6 +212,21 @@ __global__ void k_prot(Grid g, double* __restrict__ q, double gam, double rhomin
     q[7 * g.fs + c] = E;
 }
 
+// prepare_stage5 (src/ssprk.cpp:121-140) on active cells:
+// q5 = q0 + (k4/k1) q2 + (k5/k1) q3, all 8 variables.
+__global__ void k_stage5_base(Grid g, const double* __restrict__ q0, const double* __restrict__ q2,
+                              const double* __restrict__ q3, double* __restrict__ q5, double c4, double c5) {
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y, k = 3 + blockIdx.z;
+    if (i > g.nx + 2) return;
+    const long long c = g.idx(i, j, k);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        const long long o = v * g.fs + c;
+        q5[o] = q0[o] + c4 * q2[o] + c5 * q3[o];
+    }
+}
+
 __global__ void k_copy(double* __restrict__ dst, const double* __restrict__ src, long long n) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
@@ -276,6 +291,13 @@ void launch_prot(Ctx& c, int stage) {
     const Grid& g = c.g;
     k_prot<<<dim3((g.nx + 127) / 128, g.ny, g.nz), 128, 0, c.stream>>>(g, c.q[stage], c.p.gam,
                                                                       c.p.rhomin, c.p.pgmin);
+    ++c.launches;
+}
+
+void launch_stage5_base(Ctx& c, double c4, double c5) {
+    const Grid& g = c.g;
+    k_stage5_base<<<dim3((g.nx + 127) / 128, g.ny, g.nz), 128, 0, c.stream>>>(g, c.q[0], c.q[2], c.q[3], c.q[5],
+                                                                            c4, c5);
     ++c.launches;
 }
 

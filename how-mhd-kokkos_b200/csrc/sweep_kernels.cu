@@ -10,8 +10,12 @@
 // Phases of one block (tile cells c in [0, T+6), interfaces f in [0, T]; the
 // interface f sits between tile cells f+2 and f+3 and its WENO stencil is
 // cells f..f+5, src/ssprk.cpp:861-865):
-//   P0  load the 8 conserved variables of the tile, permuted to sweep order
-//       (src/ssprk.cpp:1054-1061, 1145-1152), coalesced along x
+//   P0  the 8 conserved variables of the tile (with its 3-cell halo) and the
+//       update's read operand arrive by TMA tensor loads issued one tile
+//       ahead: blocks are persistent and double-buffer the tiles, so the
+//       HBM latency of tile n+1 hides behind the arithmetic of tile n.  The
+//       variable permutation of the y/z sweeps (src/ssprk.cpp:1054-1061,
+//       1145-1152) is applied when the tile is read from shared memory.
 //   P1  per cell: primitives with floors (458-516), eigenvalues and fluxes
 //       (538-595)
 //   P2a per interface: arithmetic-mean state and the eigen-system scalars
@@ -19,25 +23,26 @@
 //   P2b per (interface, row): left-eigenvector row r and right-eigenvector
 //       column r with normalisation and sign convention (662-818); the row
 //       index is warp-uniform, so the 7 formula branches do not diverge
+//   P1b per cell: differences dU(c) = U(c+1) - U(c) of (F, q_proj)
 //   P3  per (interface pair, characteristic field m): projection of the
-//       6-cell stencil, LLF split, WENO5-JS flux (841-937).  Seven threads
-//       of a warp share a pair and read the same cells, so the shared-memory
-//       loads broadcast; two interfaces per thread reuse 5 of 7 cells.
+//       stencil's 5 cell differences, LLF split, WENO5-JS flux (841-937).
+//       Seven threads of a warp share a pair and read the same cells, so the
+//       shared-memory loads broadcast; two interfaces per thread reuse 4 of 6
+//       differences.  The central part's F_{i} share is not projected: with
+//       R L = I it is added back in physical space in P4.
 //   P4  per interface: back-projection R * F^ in m order (941-943), CT terms
 //       (967-994) stored straight to the CT flux arrays (433-456 ...)
 //   P5  per cell: -dtdl (F^_{i+1/2} - F^_{i-1/2}) (949-965) and the stage
 //       accumulation (405-431, 1067-1096, 1158-1187)
 #include "how_internal.cuh"
+#include "tma.cuh"
 
 namespace how {
 
 namespace {
 
-__constant__ int c_perm[3][8] = {{0, 1, 2, 3, 4, 5, 6, 7},
-                                 {0, 2, 3, 1, 5, 6, 4, 7},
-                                 {0, 3, 1, 2, 6, 4, 5, 7}};
 
-template <int NL, int T>
+template <int DIR, int NL, int T>
 struct Tile {
     static constexpr int C = T + 6;
     static constexpr int F = T + 1;
@@ -45,108 +50,248 @@ struct Tile {
     static constexpr int NLC = NL * C;
     static constexpr int NLF = NL * F;
     static constexpr int NI = NLF | 1;              // odd interface pitch: conflict-free banks
-    // shared-memory carve-up, in doubles
-    static constexpr int oQ = 0;                    // [8][NLC] raw conserved
-    static constexpr int oU = oQ + 8 * NLC;         // [NLC][14] F(7), q_proj(7)
-    static constexpr int oP = oU + 14 * NLC;        // [9][NLC] primitives
+    // update tile: x starts one cell early so its innermost TMA coordinate is even
+    static constexpr int TO = DIR == 0 ? T + 2 : T;
+    static constexpr int NQ = 8 * NLC;              // raw tile, TMA box order [var][...]
+    static constexpr int NO = 8 * NL * TO;          // update operand tile
+    static constexpr int NQp = (NQ + 15) / 16 * 16; // 128-byte multiples
+    static constexpr int NOp = (NO + 15) / 16 * 16;
+    // shared-memory carve-up, in doubles (base 128-byte aligned)
+    static constexpr int oQ = 0;                    // 2 x [8][...] raw conserved (double-buffered)
+    static constexpr int oO = oQ + 2 * NQp;         // [8][...] update operand of the current tile
+    static constexpr int oF = oO + NOp;             // [NLC][7] cell fluxes F
+    static constexpr int oP = oF + 7 * NLC;         // [9][NLC] primitives
     static constexpr int oA = oP + 9 * NLC;         // [7][NLC] eigenvalues
-    static constexpr int oL = oA + 7 * NLC;         // [7 row][7 col][NI] left eigenvectors
+    static constexpr int oD = oA + 7 * NLC;         // [NLC][14] U(c) = (F, q_proj), then dU(c) = U(c+1) - U(c)
+    static constexpr int oL = oD + 14 * NLC;        // [7 row][7 col][NI] left eigenvectors
     static constexpr int oR = oL + 49 * NI;         // [7 wave][7 phys][NI] right eigenvectors
     static constexpr int oS = oR + 49 * NI;         // [20][NI] scalars | Fs [7][NI], dF [7][NI]
-    static constexpr int NS = 20;
-    static constexpr int total = oS + NS * NI;
+    static constexpr int NS = 21;
+    static constexpr int oB = oS + NS * NI;         // 3 mbarriers: raw tile x2, update operand
+    static constexpr int total = oB + 3;
     static constexpr size_t bytes = sizeof(double) * (size_t)total;
+    static constexpr uint32_t in_bytes = 8u * NQ;
+    static constexpr uint32_t out_bytes = 8u * NO;
 };
 
 enum { S_VX, S_VY, S_VZ, S_BY, S_BZ, S_VV2, S_CS, S_CS2, S_LF, S_LS, S_AF, S_AS, S_BTY,
-       S_BTZ, S_SGNBX, S_SQR, S_ISQR, S_SGNBT, S_FLIP, S_BTV };
+       S_BTZ, S_SGNBX, S_SQR, S_ISQR, S_SGNBT, S_FLIP, S_BTV, S_ICS2 };
 
 __device__ __forceinline__ double sign1(double x) { return (x >= 0.0) ? 1.0 : -1.0; }
 
-// one WENO5-JS half in flux-difference form (src/ssprk.cpp:896-912).  The
-// three nonlinear weights share one division: with e_k = (eps + IS_k)^2,
-// omega0 = e1 e2 / D, omega2 = 3 e0 e1 / D, D = e1 e2 + 6 e0 e2 + 3 e0 e1.
-__device__ __forceinline__ double weno_half(double a, double b, double c, double d) {
-    const double eps = 1.0e-10;
+// Characteristic WENO5-JS/LLF flux of one field (src/ssprk.cpp:883-937) from
+// the projected cell differences dF_k = L.(F_{k+1} - F_k), dq_k = L.(q_{k+1} - q_k),
+// k = 0..4 over the 6-cell stencil.
+//
+// Restated, not transcribed:
+//  * the fourth-order central part (-F1 + 7F2 + 7F3 - F4)/12 equals
+//    F2 + (dF1 + 6 dF2 - dF3)/12; its F2 share is added back in physical
+//    space after the back-projection (R L = I), so only the correction is
+//    returned;
+//  * the LLF-split arguments 0.5 (dF +- amx dq) are used without the 0.5:
+//    doubling a, b, c, d quadruples every smoothness indicator, so with
+//    eps -> 4 eps the nonlinear weights are unchanged and the 0.5 moves onto
+//    the linear combination (1/3 -> 1/6, 1/6 -> 1/12);
+//  * omega0 = a0 / (a0 + a1 + a2) with a_k = c_k / (eps + IS_k)^2 is
+//    e1 e2 / D with e_k = (eps + IS_k)^2 and D = e1 e2 + 6 e0 e2 + 3 e0 e1
+//    (omega2 = 3 e0 e1 / D); the two halves share one division 1/(D+ D-).
+__device__ __forceinline__ void weno_terms(double a, double b, double c, double d, double& num0,
+                                           double& num2, double& den, double& l0, double& l2) {
+    const double eps4 = 4.0e-10;
     const double t0 = a - b, t1 = a - 3.0 * b;
     const double t2 = b - c, t3 = b + c;
     const double t4 = c - d, t5 = 3.0 * c - d;
-    const double IS0 = 13.0 * t0 * t0 + 3.0 * t1 * t1;
-    const double IS1 = 13.0 * t2 * t2 + 3.0 * t3 * t3;
-    const double IS2 = 13.0 * t4 * t4 + 3.0 * t5 * t5;
-    const double d0 = eps + IS0, d1 = eps + IS1, d2 = eps + IS2;
+    const double d0 = eps4 + (13.0 * t0 * t0 + 3.0 * t1 * t1);
+    const double d1 = eps4 + (13.0 * t2 * t2 + 3.0 * t3 * t3);
+    const double d2 = eps4 + (13.0 * t4 * t4 + 3.0 * t5 * t5);
     const double e0 = d0 * d0, e1 = d1 * d1, e2 = d2 * d2;
-    const double e12 = e1 * e2, e01 = e0 * e1;
-    const double inv = 1.0 / (e12 + 6.0 * (e0 * e2) + 3.0 * e01);
-    const double w0 = e12 * inv;
-    const double w2 = 3.0 * e01 * inv;
-    return w0 * (a - 2.0 * b + c) * (1.0 / 3.0) + (w2 - 0.5) * (b - 2.0 * c + d) * (1.0 / 6.0);
+    num0 = e1 * e2;
+    num2 = 3.0 * (e0 * e1);
+    den = num0 + 6.0 * (e0 * e2) + num2;
+    l0 = a - 2.0 * b + c;
+    l2 = b - 2.0 * c + d;
 }
 
-__device__ __forceinline__ double weno_flux(const double* Fsk, const double* qsk, double amx) {
-    double dF[5], dq[5];
-#pragma unroll
-    for (int s = 0; s < 5; ++s) { dF[s] = Fsk[s + 1] - Fsk[s]; dq[s] = qsk[s + 1] - qsk[s]; }
-    const double first = (-Fsk[1] + 7.0 * Fsk[2] + 7.0 * Fsk[3] - Fsk[4]) * (1.0 / 12.0);
-    const double second = weno_half(0.5 * (dF[0] + amx * dq[0]), 0.5 * (dF[1] + amx * dq[1]),
-                                    0.5 * (dF[2] + amx * dq[2]), 0.5 * (dF[3] + amx * dq[3]));
-    const double third = weno_half(0.5 * (dF[4] - amx * dq[4]), 0.5 * (dF[3] - amx * dq[3]),
-                                   0.5 * (dF[2] - amx * dq[2]), 0.5 * (dF[1] - amx * dq[1]));
+__device__ __forceinline__ double weno_flux_d(const double* dF, const double* dq, double amx) {
+    double n0p, n2p, Dp, l0p, l2p, n0m, n2m, Dm, l0m, l2m;
+    weno_terms(dF[0] + amx * dq[0], dF[1] + amx * dq[1], dF[2] + amx * dq[2], dF[3] + amx * dq[3],
+               n0p, n2p, Dp, l0p, l2p);
+    weno_terms(dF[4] - amx * dq[4], dF[3] - amx * dq[3], dF[2] - amx * dq[2], dF[1] - amx * dq[1],
+               n0m, n2m, Dm, l0m, l2m);
+    double ip, im;
+    const double DD = Dp * Dm;
+    if (DD < 1.0e300) { const double r = 1.0 / DD; ip = Dm * r; im = Dp * r; }
+    else { ip = 1.0 / Dp; im = 1.0 / Dm; }
+    const double first = (dF[1] + 6.0 * dF[2] - dF[3]) * (1.0 / 12.0);
+    const double second = (n0p * ip) * l0p * (1.0 / 6.0) + ((n2p * ip) - 0.5) * l2p * (1.0 / 12.0);
+    const double third = (n0m * im) * l0m * (1.0 / 6.0) + ((n2m * im) - 0.5) * l2m * (1.0 / 12.0);
     return first - second + third;
 }
 
+__device__ __forceinline__ constexpr int perm_of(int dir, int v) {
+    // line variable v -> conserved index (x: identity; y: rho,My,Mz,Mx,By,Bz,Bx,E;
+    // z: rho,Mz,Mx,My,Bz,Bx,By,E)
+    return dir == 0 ? v
+         : dir == 1 ? (v == 1 ? 2 : v == 2 ? 3 : v == 3 ? 1 : v == 4 ? 5 : v == 5 ? 6 : v == 6 ? 4 : v)
+                    : (v == 1 ? 3 : v == 2 ? 1 : v == 3 ? 2 : v == 4 ? 6 : v == 5 ? 4 : v == 6 ? 5 : v);
+}
+
+constexpr uint32_t kWaitLimit = 1u << 26;   // bounded TMA wait (~seconds), then flag and skip
+
 template <int DIR, int NL, int T, int NT>
-__global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
-    using TL = Tile<NL, T>;
+__global__ void __launch_bounds__(NT, 4) k_sweep(const __grid_constant__ SweepArgs a) {
+    using TL = Tile<DIR, NL, T>;
     constexpr int C = TL::C, F = TL::F, NP = TL::NP, NLC = TL::NLC, NLF = TL::NLF, NI = TL::NI;
-    extern __shared__ __align__(16) double sm[];
-    double* sQ = sm + TL::oQ;
-    double* sU = sm + TL::oU;
+    constexpr int TO = TL::TO;
+    extern __shared__ __align__(128) double sm_raw[];
+    // TMA destinations need 128-byte alignment: align the carve-up base
+    double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sm_raw) + 127) & ~uintptr_t(127));
+    double* sFc = sm + TL::oF;
     double* sP = sm + TL::oP;
     double* sA = sm + TL::oA;
+    double* sD = sm + TL::oD;
     double* sL = sm + TL::oL;
     double* sR = sm + TL::oR;
     double* sS = sm + TL::oS;
     double* sFs = sS;              // [7][NI], after P2b
     double* sdF = sS + 7 * NI;     // [7][NI], after P3
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TL::oB);
 
     const Grid& g = a.g;
     const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
     const int nt1 = DIR == 0 ? g.ny : g.nx;
+    const int nt2 = DIR == 2 ? g.ny : g.nz;
     const long long sstride = DIR == 0 ? 1ll : DIR == 1 ? (long long)g.pitch : (long long)g.pitch * g.P1;
-    const int c0 = blockIdx.x * T;                  // padded index of tile cell 0
-    const int t1_0 = 3 + blockIdx.y * NL;
-    const int t2 = 3 + blockIdx.z;
+    // Tiles: T active cells along the sweep x NL lines x one plane.  Lines of
+    // the x sweep start at j = 3; lines of the y/z sweeps are consecutive i and
+    // start at the even i = 2 (a masked ghost line) so the innermost TMA
+    // coordinate stays 16-byte aligned.
+    const int ntx = (n + T - 1) / T;
+    const int line0 = DIR == 0 ? 3 : 2;
+    const int nty = DIR == 0 ? (nt1 + NL - 1) / NL : (nt1 + 1 + NL - 1) / NL;
+    const long long ntiles = (long long)ntx * nty * nt2;
     const int tid = threadIdx.x;
-    const int Pn = n + 6;
 
-    auto line_off = [&](int l) -> long long {
-        const int t1 = t1_0 + l;
-        if (DIR == 0) return g.idx(0, t1, t2);
-        if (DIR == 1) return g.idx(t1, 0, t2);
-        return g.idx(t1, t2, 0);
-    };
-    auto line_ok = [&](int l) -> bool { return t1_0 + l <= nt1 + 2; };
-
-    // ---------------------------------------------------------------- P0
-    for (int t = tid; t < 8 * NLC; t += blockDim.x) {
-        int v, l, c;
-        if (DIR == 0) { v = t / NLC; const int r = t % NLC; l = r / C; c = r % C; }
-        else { v = t / NLC; const int r = t % NLC; c = r / NL; l = r % NL; }
-        double val = (v == 0 || v == 7) ? 1.0 : 0.0;
-        if (line_ok(l) && c0 + c < Pn)
-            val = a.qprev[(long long)c_perm[DIR][v] * g.fs + line_off(l) + (long long)(c0 + c) * sstride];
-        sQ[v * NLC + l * C + c] = val;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        fence_barrier_init();
     }
     __syncthreads();
+
+    // TMA loads (thread 0 only): the raw tile of `tile` into buffer b
+    // (which == 0) or its update operand (which == 1).
+    auto issue = [&](long long tile, int which, int b) -> bool {
+        const int tx = (int)(tile % ntx);
+        const long long r = tile / ntx;
+        const int ty = (int)(r % nty), tz = (int)(r / nty);
+        const int c0 = tx * T, t1_0 = line0 + ty * NL, t2 = 3 + tz;
+        int cc[4];
+        if (which == 0) {
+            if (DIR == 0) { cc[0] = c0; cc[1] = t1_0; cc[2] = t2; }
+            else if (DIR == 1) { cc[0] = t1_0; cc[1] = c0; cc[2] = t2; }
+            else { cc[0] = t1_0; cc[1] = t2; cc[2] = c0; }
+        } else {
+            if (DIR == 0) { cc[0] = c0 + 2; cc[1] = t1_0; cc[2] = t2; }
+            else if (DIR == 1) { cc[0] = t1_0; cc[1] = c0 + 3; cc[2] = t2; }
+            else { cc[0] = t1_0; cc[1] = t2; cc[2] = c0 + 3; }
+        }
+        cc[3] = 0;
+        if (cc[0] & 1) {   // never issue a misaligned tensor copy
+            atomicOr(a.status, HOW_STATUS_TMA_ALIGN);
+            return false;
+        }
+        fence_proxy_async_smem();
+        if (which == 0) {
+            mbar_arrive_expect_tx(&bars[b], TL::in_bytes);
+            tma_load_4d(sm + TL::oQ + b * TL::NQp, &a.tm_in, &bars[b], cc[0], cc[1], cc[2], cc[3]);
+        } else {
+            mbar_arrive_expect_tx(&bars[2], TL::out_bytes);
+            tma_load_4d(sm + TL::oO, &a.tm_out, &bars[2], cc[0], cc[1], cc[2], cc[3]);
+        }
+        return true;
+    };
+
+    long long tile = blockIdx.x;
+    int buf = 0;
+    uint32_t par_bits = 0u;    // phase parity per barrier (bit k)
+    uint32_t pend_bits = 0u;   // copies in flight per barrier (thread 0's view, bit k)
+    bool issued_ok = true;
+    if (tid == 0 && tile < ntiles) {
+        issued_ok = issue(tile, 0, 0) && issue(tile, 1, 0);
+        pend_bits = issued_ok ? 5u : 0u;
+    }
+    // On a failed wait the whole block leaves together; thread 0 first waits
+    // (bounded) for the copies it still has in flight.
+    auto bail = [&]() {
+        if (tid == 0) {
+            atomicOr(a.status, HOW_STATUS_TMA_TIMEOUT);
+            for (int k = 0; k < 3; ++k)
+                if ((pend_bits >> k) & 1u) mbar_wait_bounded(&bars[k], (par_bits >> k) & 1u, kWaitLimit);
+        }
+    };
+    // optional per-phase cycle accounting of thread 0 (a.prof != nullptr)
+    long long tprev = clock64();
+    auto mark = [&](int ph) {
+        if (a.prof != nullptr && tid == 0) {
+            const long long now = clock64();
+            atomicAdd(a.prof + ph, (unsigned long long)(now - tprev));
+            if (ph == 6) atomicAdd(a.prof + 7, 1ull);   // tiles
+            tprev = now;
+        }
+    };
+
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int tx = (int)(tile % ntx);
+        const long long rr0 = tile / ntx;
+        const int ty = (int)(rr0 % nty), tz = (int)(rr0 / nty);
+        const int c0 = tx * T;                       // padded index of tile cell 0
+        const int t1_0 = line0 + ty * NL;
+        const int t2 = 3 + tz;
+        auto line_off = [&](int l) -> long long {
+            const int t1 = t1_0 + l;
+            if (DIR == 0) return g.idx(0, t1, t2);
+            if (DIR == 1) return g.idx(t1, 0, t2);
+            return g.idx(t1, t2, 0);
+        };
+        auto line_ok = [&](int l) -> bool { return t1_0 + l >= 3 && t1_0 + l <= nt1 + 2; };
+        const double* sQ = sm + TL::oQ + buf * TL::NQp;
+        const double* sO = sm + TL::oO;
+        // raw conserved of line variable v at (line l, tile cell c); box order
+        // x: [var][line][cell], y/z: [var][cell][line]
+        auto qraw = [&](int v, int l, int c) -> double {
+            const int gv = perm_of(DIR, v);
+            return DIR == 0 ? sQ[(gv * NL + l) * C + c] : sQ[(gv * C + c) * NL + l];
+        };
+        auto oraw = [&](int gv, int l, int ct) -> double {
+            return DIR == 0 ? sO[(gv * NL + l) * TO + ct + 1] : sO[(gv * TO + ct) * NL + l];
+        };
+
+        // ------------------------------------------------------------ P0
+        {
+            const bool ok = issued_ok && mbar_wait_bounded(&bars[buf], (par_bits >> buf) & 1u, kWaitLimit);
+            if (__syncthreads_or(!ok)) { bail(); return; }   // results void; host sees the status
+        }
+        par_bits ^= 1u << buf;
+        pend_bits &= ~(1u << buf);
+        {
+            const long long next = tile + gridDim.x;
+            if (tid == 0 && next < ntiles) {
+                issued_ok = issue(next, 0, buf ^ 1) && issued_ok;
+                pend_bits |= 1u << (buf ^ 1);
+            }
+        }
+        mark(0);
 
     // ---------------------------------------------------------------- P1
     const double gam = a.gam;
     for (int t = tid; t < NLC; t += blockDim.x) {
-        const double DD = sQ[0 * NLC + t], Mx = sQ[1 * NLC + t], My = sQ[2 * NLC + t];
-        const double Mz = sQ[3 * NLC + t], Bx = sQ[4 * NLC + t], By = sQ[5 * NLC + t];
-        const double Bz = sQ[6 * NLC + t];
-        double EE = sQ[7 * NLC + t];
+        const int l = t / C, cc = t % C;
+        const double DD = qraw(0, l, cc), Mx = qraw(1, l, cc), My = qraw(2, l, cc);
+        const double Mz = qraw(3, l, cc), Bx = qraw(4, l, cc), By = qraw(5, l, cc);
+        const double Bz = qraw(6, l, cc);
+        double EE = qraw(7, l, cc);
         // primit (src/ssprk.cpp:479-512): v from the unfloored density
         double rho = DD;
         double irho = 1.0 / rho;
@@ -177,15 +322,39 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
         sA[0 * NLC + t] = vx - lf; sA[1 * NLC + t] = vx - la; sA[2 * NLC + t] = vx - ls;
         sA[3 * NLC + t] = vx;      sA[4 * NLC + t] = vx + ls; sA[5 * NLC + t] = vx + la;
         sA[6 * NLC + t] = vx + lf;
-        double* U = sU + t * 14;
-        U[0] = rho * vx;                 // DD (floored) * vx
-        U[1] = Mx * vx + pt - Bx * Bx;
-        U[2] = My * vx - Bx * By;
-        U[3] = Mz * vx - Bx * Bz;
-        U[4] = By * vx - Bx * vy;
-        U[5] = Bz * vx - Bx * vz;
-        U[6] = (EE + pt) * vx - Bx * vdB;
+        double* U = sD + t * 14;
+        double* Fc = sFc + t * 7;
+        Fc[0] = U[0] = rho * vx;                 // DD (floored) * vx
+        Fc[1] = U[1] = Mx * vx + pt - Bx * Bx;
+        Fc[2] = U[2] = My * vx - Bx * By;
+        Fc[3] = U[3] = Mz * vx - Bx * Bz;
+        Fc[4] = U[4] = By * vx - Bx * vy;
+        Fc[5] = U[5] = Bz * vx - Bx * vz;
+        Fc[6] = U[6] = (EE + pt) * vx - Bx * vdB;
         U[7] = rho; U[8] = Mx; U[9] = My; U[10] = Mz; U[11] = By; U[12] = Bz; U[13] = EE;
+    }
+    __syncthreads();
+    mark(1);
+
+    // ---------------------------------------------------------------- P1b
+    // cell differences of (F, q_proj) along each line, in place, shared by
+    // all 7 fields
+    {
+        constexpr int NIT = NLC * 14;
+        constexpr int PER = (NIT + NT - 1) / NT;
+        double dv[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int t = tid + k * NT;
+            dv[k] = 0.0;
+            if (t < NIT && (t / 14) % C + 1 < C) dv[k] = sD[t + 14] - sD[t];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int t = tid + k * NT;
+            if (t < NIT) sD[t] = dv[k];
+        }
     }
     __syncthreads();
 
@@ -235,8 +404,10 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
         S[S_SGNBT * NI] = (By != 0.0) ? sign1(By) : sign1(Bz);
         S[S_FLIP * NI] = (cs >= la) ? 1.0 : 0.0;
         S[S_BTV * NI] = bty * vy + btz * vz;
+        S[S_ICS2 * NI] = 1.0 / cs2;
     }
     __syncthreads();
+    mark(2);
 
     // ---------------------------------------------------------------- P2b
     const double gam2 = (gam - 2.0) / (gam - 1.0);
@@ -250,7 +421,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
         const double bty = S[S_BTY * NI], btz = S[S_BTZ * NI], sgnBx = S[S_SGNBX * NI];
         const double sqrtrho = S[S_SQR * NI], isqr = S[S_ISQR * NI], sgnBt = S[S_SGNBT * NI];
         const bool flip24 = S[S_FLIP * NI] != 0.0;
-        const double btv = S[S_BTV * NI];
+        const double btv = S[S_BTV * NI], ics2 = S[S_ICS2 * NI];
         double L[7], R[7];
         switch (r) {
             case 0: {
@@ -261,7 +432,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
                 L[4] = gam0 * af * By + cs * as * bty * sqrtrho;
                 L[5] = gam0 * af * Bz + cs * as * btz * sqrtrho;
                 L[6] = -gam0 * af;
-                const double s = 0.5 / cs2;
+                const double s = 0.5 * ics2;
 #pragma unroll
                 for (int m = 0; m < 7; ++m) L[m] *= s;
                 R[0] = af; R[1] = af * (vx - lf);
@@ -285,7 +456,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
                 L[4] = gam0 * as * By - cs * af * bty * sqrtrho;
                 L[5] = gam0 * as * Bz - cs * af * btz * sqrtrho;
                 L[6] = -gam0 * as;
-                const double s = 0.5 / cs2;
+                const double s = 0.5 * ics2;
 #pragma unroll
                 for (int m = 0; m < 7; ++m) L[m] *= s;
                 R[0] = as; R[1] = as * (vx - ls);
@@ -295,7 +466,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
                 break;
             }
             case 3: {
-                const double s = -gam0 / cs2;
+                const double s = -gam0 * ics2;
                 L[0] = (-cs2 / gam0 - 0.5 * vv2) * s; L[1] = vx * s; L[2] = vy * s; L[3] = vz * s;
                 L[4] = By * s; L[5] = Bz * s; L[6] = -s;
                 R[0] = 1.0; R[1] = vx; R[2] = vy; R[3] = vz; R[4] = 0.0; R[5] = 0.0; R[6] = 0.5 * vv2;
@@ -309,7 +480,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
                 L[4] = gam0 * as * By - cs * af * bty * sqrtrho;
                 L[5] = gam0 * as * Bz - cs * af * btz * sqrtrho;
                 L[6] = -gam0 * as;
-                const double s = 0.5 / cs2;
+                const double s = 0.5 * ics2;
 #pragma unroll
                 for (int m = 0; m < 7; ++m) L[m] *= s;
                 R[0] = as; R[1] = as * (vx + ls);
@@ -333,7 +504,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
                 L[4] = gam0 * af * By + cs * as * bty * sqrtrho;
                 L[5] = gam0 * af * Bz + cs * as * btz * sqrtrho;
                 L[6] = -gam0 * af;
-                const double s = 0.5 / cs2;
+                const double s = 0.5 * ics2;
 #pragma unroll
                 for (int m = 0; m < 7; ++m) L[m] *= s;
                 R[0] = af; R[1] = af * (vx + lf);
@@ -343,15 +514,16 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
                 break;
             }
         }
-        // sign convention (src/ssprk.cpp:789-818)
+        // sign convention (src/ssprk.cpp:789-818) as one factor per row/column
         const bool flip = flip24 ? (r == 2 || r == 4) : (r == 0 || r == 6);
+        const double sg = flip ? sgnBt : 1.0;
+        double* lo = sL + r * 7 * NI + i;
+        double* ro = sR + r * 7 * NI + i;
 #pragma unroll
-        for (int m = 0; m < 7; ++m) {
-            sL[(r * 7 + m) * NI + i] = flip ? L[m] * sgnBt : L[m];
-            sR[(r * 7 + m) * NI + i] = flip ? R[m] * sgnBt : R[m];
-        }
+        for (int m = 0; m < 7; ++m) { lo[m * NI] = L[m] * sg; ro[m * NI] = R[m] * sg; }
     }
     __syncthreads();
+    mark(3);
 
     // ---------------------------------------------------------------- P3
     for (int t = tid; t < 7 * NL * NP; t += blockDim.x) {
@@ -367,40 +539,45 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
             L0[v] = sL[(m * 7 + v) * NI + i0];
             L1[v] = sL[(m * 7 + v) * NI + i1];
         }
-        double Fk0[6], qk0[6], Fk1[6], qk1[6];
-        double amx0 = 0.0, amx1 = 0.0;
+        // interface f0 uses differences at cells f0..f0+4, f0+1 uses f0+1..f0+5
+        double dF0[5], dq0[5], dF1[5], dq1[5];
+        double amx0 = fabs(sA[m * NLC + l * C + f0]);
+        double amx1 = fabs(sA[m * NLC + l * C + (f0 + 1 < C ? f0 + 1 : C - 1)]);
 #pragma unroll
-        for (int cc = 0; cc < 7; ++cc) {
+        for (int cc = 0; cc < 6; ++cc) {
             int c = f0 + cc;
-            c = c < C ? c : C - 1;
-            const double2* u = reinterpret_cast<const double2*>(sU + (l * C + c) * 14);
-            double U[14];
+            c = c < C - 1 ? c : C - 2;
+            const double2* u = reinterpret_cast<const double2*>(sD + (l * C + c) * 14);
+            double D[14];
 #pragma unroll
-            for (int h = 0; h < 7; ++h) { const double2 x = u[h]; U[2 * h] = x.x; U[2 * h + 1] = x.y; }
-            const double av = fabs(sA[m * NLC + l * C + c]);
-            if (cc <= 5) {
-                double pf = L0[0] * U[0], pq = L0[0] * U[7];
+            for (int h = 0; h < 7; ++h) { const double2 x = u[h]; D[2 * h] = x.x; D[2 * h + 1] = x.y; }
+            const double av = fabs(sA[m * NLC + l * C + (c + 1)]);
+            if (cc <= 4) {
+                double pf = L0[0] * D[0], pq = L0[0] * D[7];
 #pragma unroll
-                for (int v = 1; v < 7; ++v) { pf += L0[v] * U[v]; pq += L0[v] * U[7 + v]; }
-                Fk0[cc] = pf; qk0[cc] = pq;
+                for (int v = 1; v < 7; ++v) { pf += L0[v] * D[v]; pq += L0[v] * D[7 + v]; }
+                dF0[cc] = pf; dq0[cc] = pq;
                 amx0 = fmax(amx0, av);
             }
             if (cc >= 1) {
-                double pf = L1[0] * U[0], pq = L1[0] * U[7];
+                double pf = L1[0] * D[0], pq = L1[0] * D[7];
 #pragma unroll
-                for (int v = 1; v < 7; ++v) { pf += L1[v] * U[v]; pq += L1[v] * U[7 + v]; }
-                Fk1[cc - 1] = pf; qk1[cc - 1] = pq;
+                for (int v = 1; v < 7; ++v) { pf += L1[v] * D[v]; pq += L1[v] * D[7 + v]; }
+                dF1[cc - 1] = pf; dq1[cc - 1] = pq;
                 amx1 = fmax(amx1, av);
             }
         }
-        sFs[m * NI + i0] = weno_flux(Fk0, qk0, amx0);
-        if (has1) sFs[m * NI + i1] = weno_flux(Fk1, qk1, amx1);
+        sFs[m * NI + i0] = weno_flux_d(dF0, dq0, amx0);
+        if (has1) sFs[m * NI + i1] = weno_flux_d(dF1, dq1, amx1);
     }
     __syncthreads();
+    mark(4);
 
     // ---------------------------------------------------------------- P4
     for (int t = tid; t < NLF; t += blockDim.x) {
         const int l = t / F, f = t % F;
+        const int c = l * C + f + 2;          // left cell of the interface
+        const double* F2 = sFc + c * 7;       // its physical flux (central part)
         double dF[7];
 #pragma unroll
         for (int r = 0; r < 7; ++r) dF[r] = 0.0;
@@ -411,9 +588,8 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
             for (int r = 0; r < 7; ++r) dF[r] += sR[(m * 7 + r) * NI + t] * fs;
         }
 #pragma unroll
-        for (int r = 0; r < 7; ++r) sdF[r * NI + t] = dF[r];
+        for (int r = 0; r < 7; ++r) { dF[r] += F2[r]; sdF[r * NI + t] = dF[r]; }
         // CT terms (src/ssprk.cpp:973-993): mean of B_n v_t over the two cells
-        const int c = l * C + f + 2;
         const double x1 = sP[4 * NLC + c] * sP[2 * NLC + c], x2 = sP[4 * NLC + c + 1] * sP[2 * NLC + c + 1];
         const double y1 = sP[4 * NLC + c] * sP[3 * NLC + c], y2 = sP[4 * NLC + c + 1] * sP[3 * NLC + c + 1];
         const int iface = c0 + f;   // global interface index, face at padded iface + 2
@@ -424,8 +600,15 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
         }
     }
     __syncthreads();
+    mark(5);
 
     // ---------------------------------------------------------------- P5
+    {
+        const bool ok = mbar_wait_bounded(&bars[2], (par_bits >> 2) & 1u, kWaitLimit);
+        if (__syncthreads_or(!ok)) { bail(); return; }
+    }
+    par_bits ^= 4u;
+    pend_bits &= ~4u;
     const double dtdl = *a.dtdl;
     for (int t = tid; t < 8 * NL * T; t += blockDim.x) {
         int v, l, ct;
@@ -436,44 +619,110 @@ __global__ void __launch_bounds__(NT, 4) k_sweep(SweepArgs a) {
         const int rr = v < 4 ? v : v - 1;     // flux row of line variable v (v = 4: normal B)
         const int fi = l * F + ct;
         const double delta = (v == 4) ? 0.0 : -dtdl * (sdF[rr * NI + fi + 1] - sdF[rr * NI + fi]);
-        const long long o = (long long)c_perm[DIR][v] * g.fs + line_off(l) + (long long)s * sstride;
+        const int gv = perm_of(DIR, v);
+        const long long o = (long long)gv * g.fs + line_off(l) + (long long)s * sstride;
+        const double cur = oraw(gv, l, ct);   // q(iw) (accumulate) or the RK base
         if (a.mode == 0) {
-            if (v != 4) a.qout[o] += delta;
+            if (v != 4) a.qout[o] = cur + delta;
+        } else if (a.mode == 1) {
+            a.qout[o] = a.k1 * cur + a.k3 * qraw(v, l, ct + 3) + delta;
         } else {
-            double base = a.q0[o];
-            if (a.stage5) base = base + a.c4 * a.q2[o] + a.c5 * a.q3[o];
-            if (a.mode == 1) a.qout[o] = a.k1 * base + a.k3 * sQ[v * NLC + l * C + ct + 3] + delta;
-            else a.qout[o] = base + delta;
+            a.qout[o] = cur + delta;
         }
     }
+    __syncthreads();   // every read of the update operand / raw tile is done
+    {
+        const long long next = tile + gridDim.x;
+        if (tid == 0 && next < ntiles) {
+            issued_ok = issue(next, 1, 0) && issued_ok;
+            pend_bits |= 4u;
+        }
+    }
+    mark(6);
+    buf ^= 1;
+    }   // tile loop
 }
 
 template <int DIR, int NL, int T, int NT>
 void launch_one(Ctx& c, const SweepArgs& a) {
-    using TL = Tile<NL, T>;
+    using TL = Tile<DIR, NL, T>;
     static bool attr_done = false;
     if (!attr_done) {
-        cudaFuncSetAttribute(k_sweep<DIR, NL, T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::bytes);
+        cudaFuncSetAttribute(k_sweep<DIR, NL, T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TL::bytes + 128);
         attr_done = true;
     }
     const Grid& g = c.g;
     const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
     const int nt1 = DIR == 0 ? g.ny : g.nx;
     const int nt2 = DIR == 2 ? g.ny : g.nz;
-    dim3 grid((n + T - 1) / T, (nt1 + NL - 1) / NL, nt2);
+    const long long ntx = (n + T - 1) / T;
+    const long long nty = DIR == 0 ? (nt1 + NL - 1) / NL : (nt1 + 1 + NL - 1) / NL;
+    const long long ntiles = ntx * nty * nt2;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
+    const long long resident = (long long)nsm * 4;
+    const int grid = (int)(ntiles < resident ? ntiles : resident);
     cudaEvent_t ev[2];
     timer_begin(c, ev);
-    k_sweep<DIR, NL, T, NT><<<grid, NT, TL::bytes, c.stream>>>(a);
+    k_sweep<DIR, NL, T, NT><<<grid, NT, TL::bytes + 128, c.stream>>>(a);
     timer_end(c, ev);
     ++c.launches;
 }
 
 }  // namespace
 
-void launch_sweep(Ctx& c, int dir, const SweepArgs& a) {
-    if (dir == 0) launch_one<0, 1, 32, 128>(c, a);
-    else if (dir == 1) launch_one<1, 2, 16, 128>(c, a);
-    else launch_one<2, 2, 16, 128>(c, a);
+// Sweep tile shapes: x sweeps 1 line x 32 cells, y/z sweeps 2 lines x 16 cells.
+template <int DIR> struct SweepShape;
+template <> struct SweepShape<0> { static constexpr int NL = 1, T = 32; };
+template <> struct SweepShape<1> { static constexpr int NL = 2, T = 16; };
+template <> struct SweepShape<2> { static constexpr int NL = 2, T = 16; };
+
+template <int DIR>
+static int make_maps_dir(Ctx& c) {
+    using S = SweepShape<DIR>;
+    using TL = Tile<DIR, S::NL, S::T>;
+    const Grid& g = c.g;
+    const uint64_t dims[4] = {(uint64_t)g.P0, (uint64_t)g.P1, (uint64_t)g.P2, 8};
+    const uint64_t strides[3] = {(uint64_t)g.pitch * 8, (uint64_t)g.pitch * g.P1 * 8, (uint64_t)g.fs * 8};
+    uint32_t bin[4], bout[4];
+    if (DIR == 0) { bin[0] = TL::C; bin[1] = S::NL; bin[2] = 1; bout[0] = TL::TO; bout[1] = S::NL; bout[2] = 1; }
+    else if (DIR == 1) { bin[0] = S::NL; bin[1] = TL::C; bin[2] = 1; bout[0] = S::NL; bout[1] = TL::TO; bout[2] = 1; }
+    else { bin[0] = S::NL; bin[1] = 1; bin[2] = TL::C; bout[0] = S::NL; bout[1] = 1; bout[2] = TL::TO; }
+    bin[3] = 8; bout[3] = 8;
+    for (int b = 0; b < 6; ++b) {
+        int rc = encode_tensor_map_4d(&c.tm_in[b][DIR], c.qbuf[b], dims, strides, bin);
+        if (!rc) rc = encode_tensor_map_4d(&c.tm_out[b][DIR], c.qbuf[b], dims, strides, bout);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int make_sweep_tensor_maps(Ctx& c) {
+    int rc = make_maps_dir<0>(c);
+    if (!rc) rc = make_maps_dir<1>(c);
+    if (!rc) rc = make_maps_dir<2>(c);
+    return rc;
+}
+
+static int buffer_of(const Ctx& c, const double* p) {
+    for (int b = 0; b < 6; ++b) if (c.qbuf[b] == p) return b;
+    return -1;
+}
+
+// a.qprev / a.qout / a.q0 choose the tensor maps: the tile comes from qprev;
+// the update operand is q(iw) when accumulating (mode 0) or when the base was
+// prepared in q(iw) (stage 5), else q(0).
+void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
+    SweepArgs a = a_in;
+    a.prof = c.prof;
+    a.status = &c.dsc->status;
+    const int bin = buffer_of(c, a.qprev);
+    const int bout = buffer_of(c, (a.mode == 0 || a.stage5) ? a.qout : a.q0);
+    a.tm_in = c.tm_in[bin][dir];
+    a.tm_out = c.tm_out[bout][dir];
+    if (dir == 0) launch_one<0, SweepShape<0>::NL, SweepShape<0>::T, 128>(c, a);
+    else if (dir == 1) launch_one<1, SweepShape<1>::NL, SweepShape<1>::T, 128>(c, a);
+    else launch_one<2, SweepShape<2>::NL, SweepShape<2>::T, 128>(c, a);
 }
 
 }  // namespace how

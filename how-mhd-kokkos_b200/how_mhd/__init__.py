@@ -103,6 +103,7 @@ def _load():
         "how_set_kernel_timing": ([V, ctypes.c_int], ctypes.c_int),
         "how_get_kernel_timing": ([V, D, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
         "how_measure_fp64_peak": ([D, ctypes.c_int], ctypes.c_int),
+        "how_sweep_phase_profile": ([V, ctypes.c_int, ctypes.c_double, D, ctypes.c_int], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -282,6 +283,12 @@ class Domain:
         dts = np.zeros(max(dts_cap, 1))
         _check(_lib.how_run(self._h, ctypes.byref(t), max_steps, ctypes.byref(s), _dptr(dts), dts_cap))
         return t.value, s.value, dts[: min(s.value, dts_cap)].copy()
+
+    def sweep_phase_profile(self, direction: int, dt: float):
+        """Mean cycles per block of each sweep phase (instrumentation)."""
+        out = np.zeros(8)
+        _check(_lib.how_sweep_phase_profile(self._h, direction, dt, _dptr(out), 8))
+        return out
 
     def set_precision(self, mode):
         if isinstance(mode, str):

@@ -161,6 +161,11 @@ void* how_stream(how_ctx* ctx);
 int how_set_kernel_timing(how_ctx* ctx, int on);
 /* Summed device milliseconds and count of the timed sweep launches. */
 int how_get_kernel_timing(how_ctx* ctx, double* total_ms, long* launches);
+/* Mean cycles per thread block of each phase of one stage-1 sweep (the
+ * how_sweep semantics) -- instrumentation, no reference counterpart.
+ * out[0..6] = phases (load, primitives, differences+scalars, eigenvector
+ * rows, projection+WENO, back-projection+CT, update); out[7] = blocks. */
+int how_sweep_phase_profile(how_ctx* ctx, int dir, double dt, double* out, int nout);
 /* Measured FP64 FMA-pipe throughput of the current device, TFLOP/s (2 flops
  * per FMA): the roofline denominator of this FP64-bound path. */
 int how_measure_fp64_peak(double* tflops, int reps);
