@@ -166,6 +166,31 @@ int how_get_kernel_timing(how_ctx* ctx, double* total_ms, long* launches);
  * out[0..6] = phases (load, primitives, differences+scalars, eigenvector
  * rows, projection+WENO, back-projection+CT, update); out[7] = blocks. */
 int how_sweep_phase_profile(how_ctx* ctx, int dir, double dt, double* out, int nout);
+/* ---------------------------------------------------- allocation-free use */
+/* Capacity of the fixed scratch behind how_tstep_noalloc, in (i, j) lines. */
+#define HOW_NOALLOC_MAX_LINES 262144
+
+/* CFL time step of a state the caller already holds on the GPU, without
+ * allocating any device memory.  No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- a host application whose memory
+ * pool owns the whole device (Kokkos, AMReX and similar), or code running
+ * under an allocator that forbids device allocation after set-up.
+ *   q_dev : stage 0 in the reference layout (8 x (nx+6) x (ny+6) x (nz+6)
+ *           doubles, k fastest) in device memory
+ *   p     : grid sizes, box sizes, gam, cour, rhomin, pgmin are read
+ *   dt_dev: one double in device memory that receives dt, computed as
+ *           tstep does (src/tstep.cpp:11-136)
+ *   stream: cudaStream_t to order the work on (NULL = legacy stream)
+ * The reduction keeps its partial results in one fixed device array of
+ * HOW_NOALLOC_MAX_LINES x 3 doubles (6 MiB) that every GPU loading this
+ * library holds until exit; nx * ny above HOW_NOALLOC_MAX_LINES is refused
+ * with HOW_ERR_ARG.  The first call on each device looks up that array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.  The
+ * call is asynchronous; read dt_dev after synchronising `stream`. */
+int how_tstep_noalloc(const double* q_dev, const how_params* p, double* dt_dev, void* stream);
+
 /* Measured FP64 FMA-pipe throughput of the current device, TFLOP/s (2 flops
  * per FMA): the roofline denominator of this FP64-bound path. */
 int how_measure_fp64_peak(double* tflops, int reps);
