@@ -216,6 +216,24 @@ def bench_reference(args):
     return 0
 
 
+# --------------------------------------------------------- replica helpers
+def max_over_ranks(x, world, device):
+    """Max of a per-rank scalar over all ranks (the timing rule: the slowest
+    replica sets the time).  `device` is "cuda" under NCCL, "cpu" under gloo."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, zones, steps, max_ms):
+    """Whole-job zone-cycles/s: every replica advances `zones` for `steps`."""
+    return world * zones * steps / (max_ms * 1e-3)
+
+
 # ------------------------------------------------------------------ our arm
 def load_traffic_profile(precision):
     f = REPO / "profiles" / "sweep_traffic.json"
@@ -254,13 +272,6 @@ def bench_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     # warm-up
     t_sim, s, _ = dom.run(0.0, args.warmup)
@@ -286,8 +297,8 @@ def bench_ours(args):
     hm.lib().how_get_kernel_timing(dom._h, ctypes.byref(sweep_ms), ctypes.byref(sweep_n))
     hm.lib().how_set_kernel_timing(dom._h, 0)
     clocks = sampler.stop() if sampler else None
-    ms = max_over_ranks(ms)
-    value = world * n ** 3 * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ms, world, "cuda")
+    value = replica_value(world, n ** 3, args.steps, ms)
 
     # e2e through the C ABI with pinned host buffers
     e2e = None
@@ -310,7 +321,7 @@ def bench_ours(args):
             dom.get_face_b_into(*bh)
         f1.record(stream)
         barrier()
-        ems = max_over_ranks(f0.elapsed_time(f1))
+        ems = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
         nbytes = 8 * int(np.prod(shp)) + 3 * 8 * int(np.prod(p.shape))
         e2e = {"value": world * n ** 3 * args.steps / (ems * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
