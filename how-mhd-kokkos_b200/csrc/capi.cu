@@ -13,6 +13,7 @@
 #include <vector>
 
 namespace how {
+int router_enable_default(how_ctx* c);
 
 static thread_local std::string g_err;
 
@@ -199,6 +200,7 @@ int how_create(const how_params* p, how_ctx** out) {
     if (e != cudaSuccess) { how_destroy(c); return cuda_fail(e, "context set-up"); }
     std::memset(c->hsc, 0, sizeof(DevScalars));
     if ((rc = make_sweep_tensor_maps(*c))) { how_destroy(c); return rc; }
+    if (pp.router && (rc = router_enable_default(c))) { how_destroy(c); return rc; }
     *out = c;
     return HOW_OK;
 }
@@ -208,6 +210,11 @@ int how_destroy(how_ctx* c) {
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->mem) cudaFree(c->mem);
+    if (c->router_w) cudaFree(c->router_w);
+    if (c->route_prev) cudaFree(c->route_prev);
+    if (c->route_count) cudaFree(c->route_count);
+    if (c->collect) cudaFree(c->collect);
+    if (c->collect_n) cudaFree(c->collect_n);
     if (c->dsc) cudaFree(c->dsc);
     if (c->hsc) cudaFreeHost(c->hsc);
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -77,9 +77,36 @@ struct SweepArgs {
     double k1, k3, c4, c5; // c4 = k4 / k1, c5 = k5 / k1
     int mode;              // 0 accumulate, 1 first sweep with RK combine, 2 first sweep base+delta
     int stage5;            // base = q0 + c4 q2 + c5 q3
+    int ct4;               // 4-point face average of B_n v_t in the CT terms (else 2-point)
     double gam, rhomin, pgmin;
     unsigned long long* prof;   // optional per-phase cycle counters (instrumentation)
     unsigned int* status;       // device status word (HOW_STATUS_* bits)
+    // learned routing (MODE 1/2) and label collection (MODE 3)
+    const float* router;        // packed MLP weights (RouterLayout), FP32
+    const unsigned char* route_prev;  // per face: 1 if sent to full WENO by this direction's previous sweep
+    unsigned char* route_next;        // this sweep's decisions (the two arrays swap every sweep)
+    unsigned long long* route_count;   // [0] full, [1] cheap interfaces (active faces)
+    float* collect;             // records of 8 floats: 6 features, label, weight deviation
+    unsigned int* collect_n;    // records written
+    unsigned int collect_cap;   // buffer capacity (records)
+    unsigned int collect_every; // sample 1 tile in N
+    float route_thr;            // logit threshold for full WENO
+    float guard_jump;           // hard guard: relative jump of rho or p above this -> full WENO
+    float guard_floor;          // hard guard: rho or p below this multiple of the floors -> full WENO
+    // batched ensembles (ENS kernels): member m's arguments for this launch
+    // are ens_tab[m * ens_stride + ens_off + ens_par[m]]
+    const SweepArgs* ens_tab;
+    const long long* ens_tile_start;   // [ens_n + 1]: prefix of the members' tile counts
+    const int* ens_par;                // per member: stage-0 / stage-5 buffer parity
+    const int* ens_active;             // per member: 1 while it is stepping
+    int ens_n, ens_stride, ens_off;
+};
+
+// Packed router weights (FP32): W1[32][6], b1[32], W2[32][32], b2[32], w3[32], b3.
+struct RouterLayout {
+    static constexpr int H = 32, NF = 6;
+    static constexpr int oW1 = 0, ob1 = oW1 + H * NF, oW2 = ob1 + H, ob2 = oW2 + H * H, ow3 = ob2 + H,
+                         ob3 = ow3 + H, total = ob3 + 1;
 };
 
 struct Ctx {
@@ -102,6 +129,16 @@ struct Ctx {
     int precision = HOW_PREC_FP64;
     bool have_state = false;
     unsigned long long* prof = nullptr;   // device phase counters while profiling
+    // learned routing
+    int route_mode = 0;                   // 0 off, 1 learned, 2 guard only, 3 collect labels
+    float* router_w = nullptr;            // device RouterLayout weights
+    unsigned char* route_prev = nullptr;  // 3 directions x 2 (read / write) x fs bytes
+    int route_par[3] = {0, 0, 0};         // which of a direction's two arrays is read next
+    unsigned long long* route_count = nullptr;
+    float* collect = nullptr;
+    unsigned int* collect_n = nullptr;
+    unsigned int collect_cap = 0, collect_every = 1;
+    float route_thr = 0.0f, guard_jump = 0.25f, guard_floor = 100.0f;
 };
 
 // ---- kernels / launchers (defined in the .cu files) ------------------------

@@ -87,6 +87,13 @@ int parse_stream(std::istream& in, how_params* p) {
                 else if (sval == "on" || sval == "1") p->router = 1;
                 else { how::set_error("unknown router %s (off|on)", sval.c_str()); return HOW_ERR_PARSE; }
             }
+        } else if (key == "ct_avg") {
+            int v = 0;
+            ok = read_value(in, v);
+            if (ok) {
+                if (v != 2 && v != 4) { how::set_error("ct_avg must be 2 or 4, got %d", v); return HOW_ERR_PARSE; }
+                p->ct_avg = v;
+            }
         } else if (key == "seed") {
             unsigned long long s = 0;
             ok = read_value(in, s);
@@ -124,6 +131,7 @@ int how_params_default(how_params* p) {
     std::snprintf(p->output_format, sizeof(p->output_format), "dat");
     p->precision = HOW_PREC_FP64;
     p->router = 0;
+    p->ct_avg = 2;
     p->seed = 12345;
     return HOW_OK;
 }

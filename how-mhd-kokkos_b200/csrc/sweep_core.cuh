@@ -1,0 +1,1003 @@
+// sweep_core.cuh -- the fused directional sweep kernel: one launch per x/y/z
+// sweep of an SSPRK stage (src/ssprk.cpp:1000-1025, 1218-1272).  Included by
+// sweep_kernels.cu (single-domain launches) and ensemble_sweep.cu (batched
+// ensembles); each translation unit instantiates the shapes it launches.
+//
+// The reference runs a sweep as six all-line kernels with workspaces in
+// memory (qx, ux, ax, Fx and the 7x7 L and R per interface: ~18 GB at 256^3).
+// Here one thread block owns a pencil tile of NL lines x T active cells and
+// keeps every intermediate in shared memory; HBM sees only the stage input,
+// the RK base, the stage output and the two CT flux arrays.
+//
+// Phases of one block (tile cells c in [0, T+6), interfaces f in [0, T]; the
+// interface f sits between tile cells f+2 and f+3 and its WENO stencil is
+// cells f..f+5, src/ssprk.cpp:861-865):
+//   P0  the 8 conserved variables of the tile (with its 3-cell halo) and the
+//       update's read operand arrive by TMA tensor loads issued one tile
+//       ahead: blocks are persistent and double-buffer the tiles, so the
+//       HBM latency of tile n+1 hides behind the arithmetic of tile n.  The
+//       variable permutation of the y/z sweeps (src/ssprk.cpp:1054-1061,
+//       1145-1152) is applied when the tile is read from shared memory.
+//   P1  per cell: primitives with floors (458-516), eigenvalues and fluxes
+//       (538-595)
+//   P1b per cell: differences dU(c) = U(c+1) - U(c) of (F, q_proj)
+//   P2a per interface: arithmetic-mean state and the eigen-system scalars
+//       (610-660)
+//   P2b per (interface, row): left-eigenvector row r and right-eigenvector
+//       column r with normalisation and sign convention (662-818); the row
+//       index is warp-uniform, so the 7 formula branches do not diverge
+//   P3  per (interface pair, characteristic field m): projection of the
+//       stencil's 5 cell differences, LLF split, WENO5-JS flux (841-937).
+//       Seven threads of a warp share a pair and read the same cells, so the
+//       shared-memory loads broadcast; two interfaces per thread reuse 4 of 6
+//       differences.  The central part's F_{i} share is not projected: with
+//       R L = I it is added back in physical space in P4.
+//   P4  per interface: back-projection R * F^ in m order (941-943), CT terms
+//       (967-994) stored straight to the CT flux arrays (433-456 ...)
+//   P5  per cell: -dtdl (F^_{i+1/2} - F^_{i-1/2}) (949-965) and the stage
+//       accumulation (405-431, 1067-1096, 1158-1187)
+//
+// Precision: the kernel is a template on the working type R of the
+// eigen-system, projection and WENO arithmetic (P2a-P4's characteristic part).
+// R = double is the plain method.  R = float is the mixed-precision method:
+// primitives, cell fluxes, the physical central flux F_i, the back-projected
+// interface flux sum, the CT terms and the stage update stay FP64; the FP32
+// part only carries the characteristic upwind corrections, computed from cell
+// differences that are formed in FP64 and then rounded.
+#pragma once
+
+#include "how_internal.cuh"
+#include "router.cuh"
+#include "tma.cuh"
+
+#include <type_traits>
+
+namespace how {
+
+namespace {
+
+template <typename R> struct Math;
+template <> struct Math<double> {
+    using V2 = double2;
+    static __device__ __forceinline__ double sq(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+};
+template <> struct Math<float> {
+    using V2 = float2;
+    static __device__ __forceinline__ float sq(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+};
+
+__host__ __device__ constexpr int align_up(int x, int a) { return (x + a - 1) / a * a; }
+
+template <int DIR, int NL, int T, typename R>
+struct Tile {
+    static constexpr int C = T + 6;
+    static constexpr int F = T + 1;
+    static constexpr int NP = (F + 1) / 2;
+    static constexpr int NLC = NL * C;
+    static constexpr int NLF = NL * F;
+    static constexpr int NI = NLF | 1;              // odd interface pitch: conflict-free banks
+    // update tile: x starts one cell early so its innermost TMA coordinate is even
+    static constexpr int TO = DIR == 0 ? T + 2 : T;
+    static constexpr int NQ = 8 * NLC;              // raw tile, TMA box order [var][...]
+    static constexpr int NO = 8 * NL * TO;          // update operand tile
+    static constexpr int NS = 21;                   // eigen-system scalars per interface
+    // byte offsets (base 128-byte aligned; TMA destinations on 128 B)
+    static constexpr int bQ = 0;                                   // 2 x [8][..] raw conserved, FP64
+    static constexpr int bO = bQ + 2 * align_up(8 * NQ, 128);      // [8][..] update operand, FP64
+    static constexpr int bFc = bO + align_up(8 * NO, 128);         // [NLC][7] cell fluxes, FP64
+    static constexpr int bP = bFc + align_up(8 * 7 * NLC, 16);     // [9][NLC] primitives, FP64
+    static constexpr int bA = bP + align_up(8 * 9 * NLC, 16);      // [7][NLC] eigenvalues, R
+    static constexpr int bD = bA + align_up((int)sizeof(R) * 7 * NLC, 16);  // [NLC][14] dU, R
+    // L and R; before P2b this region stages U = (F, q_proj) in FP64 for P1b
+    static constexpr int szLR = (int)sizeof(R) * 98 * NI;
+    static constexpr int bL = bD + align_up((int)sizeof(R) * 14 * NLC, 16);
+    static constexpr int bR = bL + (int)sizeof(R) * 49 * NI;
+    // scalars; after P2b: Fs [7][NI] (R) then dF [7][NI] (FP64)
+    static constexpr int bS = bL + align_up(szLR > 8 * 14 * NLC ? szLR : 8 * 14 * NLC, 16);
+    static constexpr int offdF = align_up((int)sizeof(R) * 7 * NI, 8);
+    static constexpr int szS0 = (int)sizeof(R) * NS * NI;
+    static constexpr int szS1 = offdF + 8 * 7 * NI;
+    static constexpr int bB = bS + align_up(szS0 > szS1 ? szS0 : szS1, 16);   // 3 mbarriers
+    // routing (MODE 1-3): decision, compacted list, weight deviation, FP32
+    // features of the tile's interfaces, the network; BF16 features and logits
+    // of the routing phase live in the L/R region (free between P1b and P2b)
+    static constexpr int NRp = align_up(NLF, 16);                 // MMA row padding
+    static constexpr int bDec = bB + 32;                          // [NLF] int
+    static constexpr int bList = bDec + align_up(4 * NLF, 16);    // [NRp] int
+    static constexpr int bDev = bList + align_up(4 * NRp, 16);    // [NLF] float (bits)
+    static constexpr int bFt = bDev + align_up(4 * NLF, 16);      // [NLF][6] float
+    static constexpr int bRS = bFt + align_up(4 * 6 * NLF, 16);   // RouterSmem
+    static constexpr int bX = bL;                                 // [NRp][16] bf16 (aliases L/R)
+    static constexpr int bLogit = bL + align_up(2 * 16 * NRp, 16); // [NRp] float (aliases L/R)
+    static constexpr size_t bytes_plain = (size_t)bB + 3 * 8;
+    static constexpr size_t bytes_route = (size_t)bRS + sizeof(RouterSmem);
+    static_assert(2 * 16 * NRp + 4 * NRp <= szLR, "routing scratch must fit the L/R region");
+    static constexpr uint32_t in_bytes = 8u * NQ;
+    static constexpr uint32_t out_bytes = 8u * NO;
+};
+
+enum { S_VX, S_VY, S_VZ, S_BY, S_BZ, S_VV2, S_CS, S_CS2, S_LF, S_LS, S_AF, S_AS, S_BTY,
+       S_BTZ, S_SGNBX, S_SQR, S_ISQR, S_SGNBT, S_FLIP, S_BTV, S_ICS2 };
+
+template <typename R>
+__device__ __forceinline__ R sign1(R x) { return (x >= R(0)) ? R(1) : R(-1); }
+
+// Characteristic WENO5-JS/LLF flux of one field (src/ssprk.cpp:883-937) from
+// the projected cell differences dF_k = L.(F_{k+1} - F_k), dq_k = L.(q_{k+1} - q_k),
+// k = 0..4 over the 6-cell stencil.
+//
+// Restated, not transcribed:
+//  * the fourth-order central part (-F1 + 7F2 + 7F3 - F4)/12 equals
+//    F2 + (dF1 + 6 dF2 - dF3)/12; its F2 share is added back in physical
+//    space after the back-projection (R L = I), so only the correction is
+//    returned;
+//  * the LLF-split arguments 0.5 (dF +- amx dq) are used without the 0.5:
+//    doubling a, b, c, d quadruples every smoothness indicator, so with
+//    eps -> 4 eps the nonlinear weights are unchanged and the 0.5 moves onto
+//    the linear combination (1/3 -> 1/6, 1/6 -> 1/12);
+//  * FP64: omega0 = a0 / (a0 + a1 + a2) with a_k = c_k / (eps + IS_k)^2 is
+//    e1 e2 / D with e_k = (eps + IS_k)^2 and D = e1 e2 + 6 e0 e2 + 3 e0 e1
+//    (omega2 = 3 e0 e1 / D); the two halves share one division 1/(D+ D-).
+//    FP32 keeps the a_k form (the products of e_k would underflow) with fast
+//    reciprocals.
+template <typename R>
+__device__ __forceinline__ R weno_half_w(R a, R b, R c, R d, R& w0, R& w2) {
+    const R eps4 = R(4.0e-10);
+    const R t0 = a - b, t1 = a - R(3) * b;
+    const R t2 = b - c, t3 = b + c;
+    const R t4 = c - d, t5 = R(3) * c - d;
+    const R d0 = eps4 + (R(13) * t0 * t0 + R(3) * t1 * t1);
+    const R d1 = eps4 + (R(13) * t2 * t2 + R(3) * t3 * t3);
+    const R d2 = eps4 + (R(13) * t4 * t4 + R(3) * t5 * t5);
+    if constexpr (std::is_same<R, double>::value) {
+        const R e0 = d0 * d0, e1 = d1 * d1, e2 = d2 * d2;
+        w0 = e1 * e2;                       // numerators; the caller divides by D
+        w2 = R(3) * (e0 * e1);
+        return w0 + R(6) * (e0 * e2) + w2;  // D
+    } else {
+        const R a0 = Math<R>::rcp(d0 * d0);
+        const R a1 = R(6) * Math<R>::rcp(d1 * d1);
+        const R a2 = R(3) * Math<R>::rcp(d2 * d2);
+        const R is = Math<R>::rcp(a0 + a1 + a2);
+        w0 = a0 * is;
+        w2 = a2 * is;
+        return R(1);
+    }
+}
+
+template <typename R, bool DEV = false>
+__device__ __forceinline__ R weno_flux_d(const R* dF, const R* dq, R amx, R* dev = nullptr) {
+    const R ap = dF[0] + amx * dq[0], bp = dF[1] + amx * dq[1], cp = dF[2] + amx * dq[2], dp = dF[3] + amx * dq[3];
+    const R am = dF[4] - amx * dq[4], bm = dF[3] - amx * dq[3], cm = dF[2] - amx * dq[2], dm = dF[1] - amx * dq[1];
+    R w0p, w2p, w0m, w2m;
+    const R Dp = weno_half_w(ap, bp, cp, dp, w0p, w2p);
+    const R Dm = weno_half_w(am, bm, cm, dm, w0m, w2m);
+    if constexpr (std::is_same<R, double>::value) {
+        double ip, im;
+        const double DD = Dp * Dm;
+        if (DD < 1.0e300) { const double r = 1.0 / DD; ip = Dm * r; im = Dp * r; }
+        else { ip = 1.0 / Dp; im = 1.0 / Dm; }
+        w0p *= ip; w2p *= ip; w0m *= im; w2m *= im;
+    }
+    if constexpr (DEV) {
+        // largest departure of the nonlinear weights from the linear (0.1, 0.6, 0.3)
+        const R w1p = R(1) - w0p - w2p, w1m = R(1) - w0m - w2m;
+        R d = fabs(w0p - R(0.1));
+        d = fmax(d, fabs(w1p - R(0.6))); d = fmax(d, fabs(w2p - R(0.3)));
+        d = fmax(d, fabs(w0m - R(0.1))); d = fmax(d, fabs(w1m - R(0.6))); d = fmax(d, fabs(w2m - R(0.3)));
+        *dev = d;
+    }
+    const R first = (dF[1] + R(6) * dF[2] - dF[3]) * R(1.0 / 12.0);
+    const R second = w0p * (ap - R(2) * bp + cp) * R(1.0 / 6.0) + (w2p - R(0.5)) * (bp - R(2) * cp + dp) * R(1.0 / 12.0);
+    const R third = w0m * (am - R(2) * bm + cm) * R(1.0 / 6.0) + (w2m - R(0.5)) * (bm - R(2) * cm + dm) * R(1.0 / 12.0);
+    return first - second + third;
+}
+
+// Component-wise fifth-order upwind flux with the linear weights
+// (0.1, 0.6, 0.3) and a global Lax-Friedrichs speed: the cheap flux a
+// router sends smooth interfaces to.  dF_k, dq_k are the physical cell
+// differences of one component over the stencil; returns the correction to
+// the central F_i (same form as weno_flux_d, no characteristic projection).
+template <typename R>
+__device__ __forceinline__ R linear_flux_d(const R* dF, const R* dq, R amx) {
+    const R ap = dF[0] + amx * dq[0], bp = dF[1] + amx * dq[1], cp = dF[2] + amx * dq[2], dp = dF[3] + amx * dq[3];
+    const R am = dF[4] - amx * dq[4], bm = dF[3] - amx * dq[3], cm = dF[2] - amx * dq[2], dm = dF[1] - amx * dq[1];
+    const R first = (dF[1] + R(6) * dF[2] - dF[3]) * R(1.0 / 12.0);
+    const R second = R(0.1) * (ap - R(2) * bp + cp) * R(1.0 / 6.0) + R(-0.2) * (bp - R(2) * cp + dp) * R(1.0 / 12.0);
+    const R third = R(0.1) * (am - R(2) * bm + cm) * R(1.0 / 6.0) + R(-0.2) * (bm - R(2) * cm + dm) * R(1.0 / 12.0);
+    return first - second + third;
+}
+
+__device__ __forceinline__ constexpr int perm_of(int dir, int v) {
+    // line variable v -> conserved index (x: identity; y: rho,My,Mz,Mx,By,Bz,Bx,E;
+    // z: rho,Mz,Mx,My,Bz,Bx,By,E)
+    return dir == 0 ? v
+         : dir == 1 ? (v == 1 ? 2 : v == 2 ? 3 : v == 3 ? 1 : v == 4 ? 5 : v == 5 ? 6 : v == 6 ? 4 : v)
+                    : (v == 1 ? 3 : v == 2 ? 1 : v == 3 ? 2 : v == 4 ? 6 : v == 5 ? 4 : v == 6 ? 5 : v);
+}
+
+constexpr uint32_t kWaitLimit = 1u << 26;   // bounded TMA wait (~seconds), then flag and skip
+
+// MODE 0: plain method.  1: learned routing (network + guard).  2: guard-only
+// routing (the ablation).  3: plain method that also records features and
+// nonlinear-weight labels of sampled tiles for training.
+//
+// ENS: one launch advances this sweep for every member of a batched
+// ensemble; the global tile index runs over the members' tiles in order, and
+// each tile reads its member's arguments from the ensemble table.
+template <int DIR, int NL, int T, int NT, typename R, int MINB, int MODE, bool ENS = false>
+__global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ SweepArgs a0) {
+    static_assert(!ENS || MODE == 0, "ensembles run the plain method");
+    constexpr bool ROUTED = MODE == 1 || MODE == 2;
+    using TL = Tile<DIR, NL, T, R>;
+    using V2 = typename Math<R>::V2;
+    constexpr int C = TL::C, F = TL::F, NP = TL::NP, NLC = TL::NLC, NLF = TL::NLF, NI = TL::NI;
+    constexpr int TO = TL::TO;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // TMA destinations need 128-byte alignment: align the carve-up base
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    double* sFc = reinterpret_cast<double*>(sm + TL::bFc);
+    double* sP = reinterpret_cast<double*>(sm + TL::bP);
+    R* sA = reinterpret_cast<R*>(sm + TL::bA);
+    R* sD = reinterpret_cast<R*>(sm + TL::bD);
+    R* sL = reinterpret_cast<R*>(sm + TL::bL);
+    R* sR = reinterpret_cast<R*>(sm + TL::bR);
+    double* sUst = reinterpret_cast<double*>(sm + TL::bL);   // U staging (P1 -> P1b), FP64
+    R* sS = reinterpret_cast<R*>(sm + TL::bS);
+    R* sFs = sS;                                                       // [7][NI], after P2b
+    double* sdF = reinterpret_cast<double*>(sm + TL::bS + TL::offdF);   // [7][NI], after P3
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TL::bB);
+    int* sDec = reinterpret_cast<int*>(sm + TL::bDec);          // 1: full WENO, 0: linear flux
+    int* sList = reinterpret_cast<int*>(sm + TL::bList);        // full-WENO interfaces, compacted
+    float* sDev = reinterpret_cast<float*>(sm + TL::bDev);      // weight deviation (collect)
+    float* sFt = reinterpret_cast<float*>(sm + TL::bFt);        // features (collect)
+    RouterSmem* sRS = reinterpret_cast<RouterSmem*>(sm + TL::bRS);
+    __nv_bfloat16 (*sX)[16] = reinterpret_cast<__nv_bfloat16 (*)[16]>(sm + TL::bX);
+    float* sLogit = reinterpret_cast<float*>(sm + TL::bLogit);
+    __shared__ int s_nfull;
+    __shared__ unsigned int s_cnt[2];
+
+    // Tiles: T active cells along the sweep x NL lines x one plane.  Lines of
+    // the x sweep start at j = 3; lines of the y/z sweeps are consecutive i and
+    // start at the even i = 2 (a masked ghost line) so the innermost TMA
+    // coordinate stays 16-byte aligned.
+    struct Geo { int n, nt1, ntx, nty; long long sstride; };
+    auto geo_of = [](const Grid& g) -> Geo {
+        Geo o;
+        o.n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
+        o.nt1 = DIR == 0 ? g.ny : g.nx;
+        o.sstride = DIR == 0 ? 1ll : DIR == 1 ? (long long)g.pitch : (long long)g.pitch * g.P1;
+        o.ntx = (o.n + T - 1) / T;
+        o.nty = DIR == 0 ? (o.nt1 + NL - 1) / NL : (o.nt1 + 1 + NL - 1) / NL;
+        return o;
+    };
+    const int line0 = DIR == 0 ? 3 : 2;
+    // global tile -> member (ENS) and the member's arguments + local tile
+    auto member_of = [&](long long tile) -> int {
+        int lo = 0, hi = a0.ens_n - 1;   // last member whose first tile is <= tile
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a0.ens_tile_start[mid] <= tile) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    };
+    // (a __grid_constant__ parameter may be addressed: it is not copied)
+    auto args_of = [&](long long tile, long long& lt) -> const SweepArgs* {
+        if constexpr (ENS) {
+            const int m = member_of(tile);
+            lt = tile - a0.ens_tile_start[m];
+            return a0.ens_tab + ((long long)m * a0.ens_stride + a0.ens_off + a0.ens_par[m]);
+        } else {
+            lt = tile;
+            return &a0;
+        }
+    };
+    long long ntiles;
+    if constexpr (ENS) {
+        ntiles = a0.ens_tile_start[a0.ens_n];
+    } else {
+        const Geo G = geo_of(a0.g);
+        const int nt2 = DIR == 2 ? a0.g.ny : a0.g.nz;
+        ntiles = (long long)G.ntx * G.nty * nt2;
+    }
+    // the first tile at or after t (stepping by the grid) of a member that is
+    // stepping; members that reached their end time are skipped whole
+    auto advance = [&](long long t) -> long long {
+        if constexpr (ENS) {
+            while (t < ntiles) {
+                const int m = member_of(t);
+                if (a0.ens_active[m]) return t;
+                const long long end = a0.ens_tile_start[m + 1];
+                t += (end - t + gridDim.x - 1) / gridDim.x * gridDim.x;
+            }
+        }
+        return t;
+    };
+    const int tid = threadIdx.x;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        fence_barrier_init();
+    }
+    // MODE 1: the network in shared memory, and its logits for a flat stencil
+    // (every jump feature at its floor) with prior 0 and 1: rows of a tile
+    // whose 16 interfaces are all flat take these instead of a tensor-core
+    // pass (the MMA rows are independent, so the values are the same)
+    __shared__ float s_flat_logit[2];
+    float flat_feature = 0.0f;
+    if constexpr (MODE == 1) {
+        flat_feature = log10f(1e-6f + 0.0f);
+        router_load_smem(sRS, a0.router, tid, blockDim.x);
+        __syncthreads();
+        if (tid < 32) {
+            __nv_bfloat16 (*X)[16] = reinterpret_cast<__nv_bfloat16 (*)[16]>(sm + TL::bX);
+            float* lg = reinterpret_cast<float*>(sm + TL::bLogit);
+            for (int e = tid; e < 256; e += 32) {
+                const int r = e / 16, k = e % 16;
+                X[r][k] = __float2bfloat16_rn(k < 5 ? flat_feature : k == 5 ? (float)(r & 1) : 0.0f);
+            }
+            __syncwarp();
+            router_mma_16rows(sRS, X, lg);
+            __syncwarp();
+            if (tid < 2) s_flat_logit[tid] = lg[tid];
+        }
+    }
+    __syncthreads();
+
+    // TMA loads (thread 0 only): the raw tile of `tile` into buffer b
+    // (which == 0) or its update operand (which == 1).
+    auto issue = [&](long long gtile, int which, int b) -> bool {
+        long long tile;
+        const SweepArgs& a = *args_of(gtile, tile);
+        const Geo G = geo_of(a.g);
+        const int ntx = G.ntx, nty = G.nty;
+        const int tx = (int)(tile % ntx);
+        const long long r = tile / ntx;
+        const int ty = (int)(r % nty), tz = (int)(r / nty);
+        const int c0 = tx * T, t1_0 = line0 + ty * NL, t2 = 3 + tz;
+        int cc[4];
+        if (which == 0) {
+            if (DIR == 0) { cc[0] = c0; cc[1] = t1_0; cc[2] = t2; }
+            else if (DIR == 1) { cc[0] = t1_0; cc[1] = c0; cc[2] = t2; }
+            else { cc[0] = t1_0; cc[1] = t2; cc[2] = c0; }
+        } else {
+            if (DIR == 0) { cc[0] = c0 + 2; cc[1] = t1_0; cc[2] = t2; }
+            else if (DIR == 1) { cc[0] = t1_0; cc[1] = c0 + 3; cc[2] = t2; }
+            else { cc[0] = t1_0; cc[1] = t2; cc[2] = c0 + 3; }
+        }
+        cc[3] = 0;
+        if (cc[0] & 1) {   // never issue a misaligned tensor copy
+            atomicOr(a.status, HOW_STATUS_TMA_ALIGN);
+            return false;
+        }
+        fence_proxy_async_smem();
+        if (which == 0) {
+            mbar_arrive_expect_tx(&bars[b], TL::in_bytes);
+            tma_load_4d(sm + TL::bQ + b * align_up(8 * TL::NQ, 128), &a.tm_in, &bars[b], cc[0], cc[1], cc[2], cc[3]);
+        } else {
+            mbar_arrive_expect_tx(&bars[2], TL::out_bytes);
+            tma_load_4d(sm + TL::bO, &a.tm_out, &bars[2], cc[0], cc[1], cc[2], cc[3]);
+        }
+        return true;
+    };
+
+    long long tile = advance(blockIdx.x);
+    int buf = 0;
+    uint32_t par_bits = 0u;    // phase parity per barrier (bit k)
+    uint32_t pend_bits = 0u;   // copies in flight per barrier (thread 0's view, bit k)
+    bool issued_ok = true;
+    if (tid == 0 && tile < ntiles) {
+        issued_ok = issue(tile, 0, 0) && issue(tile, 1, 0);
+        pend_bits = issued_ok ? 5u : 0u;
+    }
+    // On a failed wait the whole block leaves together; thread 0 first waits
+    // (bounded) for the copies it still has in flight.
+    auto bail = [&]() {
+        if (tid == 0) {
+            atomicOr(a0.status, HOW_STATUS_TMA_TIMEOUT);
+            for (int k = 0; k < 3; ++k)
+                if ((pend_bits >> k) & 1u) mbar_wait_bounded(&bars[k], (par_bits >> k) & 1u, kWaitLimit);
+        }
+    };
+    // optional per-phase cycle accounting of thread 0 (prof != nullptr)
+    long long tprev = clock64();
+    auto mark = [&](int ph) {
+        if (a0.prof != nullptr && tid == 0) {
+            const long long now = clock64();
+            atomicAdd(a0.prof + ph, (unsigned long long)(now - tprev));
+            if (ph == 6) atomicAdd(a0.prof + 7, 1ull);   // tiles
+            tprev = now;
+        }
+    };
+    for (; tile < ntiles; tile = advance(tile + gridDim.x)) {
+        long long ltile;
+        const SweepArgs& a = *args_of(tile, ltile);
+        const Grid& g = a.g;
+        const Geo G = geo_of(g);
+        const int n = G.n, nt1 = G.nt1, ntx = G.ntx, nty = G.nty;
+        const long long sstride = G.sstride;
+        const double gam = a.gam;
+        const R gamR = R(a.gam);
+        const R gam0 = R(1) - gamR, gam1 = R(0.5) * (gamR - R(1));
+        const R gam2 = (gamR - R(2)) / (gamR - R(1));
+        const int tx = (int)(ltile % ntx);
+        const long long rr0 = ltile / ntx;
+        const int ty = (int)(rr0 % nty), tz = (int)(rr0 / nty);
+        const int c0 = tx * T;                       // padded index of tile cell 0
+        const int t1_0 = line0 + ty * NL;
+        const int t2 = 3 + tz;
+        auto line_off = [&](int l) -> long long {
+            const int t1 = t1_0 + l;
+            if (DIR == 0) return g.idx(0, t1, t2);
+            if (DIR == 1) return g.idx(t1, 0, t2);
+            return g.idx(t1, t2, 0);
+        };
+        auto line_ok = [&](int l) -> bool { return t1_0 + l >= 3 && t1_0 + l <= nt1 + 2; };
+        const double* sQ = reinterpret_cast<const double*>(sm + TL::bQ + buf * align_up(8 * TL::NQ, 128));
+        const double* sO = reinterpret_cast<const double*>(sm + TL::bO);
+        // raw conserved of line variable v at (line l, tile cell c); box order
+        // x: [var][line][cell], y/z: [var][cell][line]
+        auto qraw = [&](int v, int l, int c) -> double {
+            const int gv = perm_of(DIR, v);
+            return DIR == 0 ? sQ[(gv * NL + l) * C + c] : sQ[(gv * C + c) * NL + l];
+        };
+        auto oraw = [&](int gv, int l, int ct) -> double {
+            return DIR == 0 ? sO[(gv * NL + l) * TO + ct + 1] : sO[(gv * TO + ct) * NL + l];
+        };
+
+        // ------------------------------------------------------------ P0
+        {
+            const bool ok = issued_ok && mbar_wait_bounded(&bars[buf], (par_bits >> buf) & 1u, kWaitLimit);
+            if (__syncthreads_or(!ok)) { bail(); return; }   // results void; host sees the status
+        }
+        par_bits ^= 1u << buf;
+        pend_bits &= ~(1u << buf);
+        {
+            const long long next = advance(tile + gridDim.x);
+            if (tid == 0 && next < ntiles) {
+                issued_ok = issue(next, 0, buf ^ 1) && issued_ok;
+                pend_bits |= 1u << (buf ^ 1);
+            }
+        }
+        mark(0);
+
+        // ------------------------------------------------------------ P1
+        for (int t = tid; t < NLC; t += blockDim.x) {
+            const int l = t / C, cc = t % C;
+            const double DD = qraw(0, l, cc), Mx = qraw(1, l, cc), My = qraw(2, l, cc);
+            const double Mz = qraw(3, l, cc), Bx = qraw(4, l, cc), By = qraw(5, l, cc);
+            const double Bz = qraw(6, l, cc);
+            double EE = qraw(7, l, cc);
+            // primit (src/ssprk.cpp:479-512): v from the unfloored density
+            double rho = DD;
+            double irho = 1.0 / rho;
+            const double vx = Mx * irho, vy = My * irho, vz = Mz * irho;
+            const double vv2 = vx * vx + vy * vy + vz * vz;
+            const double BB2 = Bx * Bx + By * By + Bz * Bz;
+            double pg = (gam - 1.0) * (EE - 0.5 * (rho * vv2 + BB2));
+            if (rho < a.rhomin || pg < a.pgmin) {
+                rho = fmax(a.rhomin, rho);
+                pg = fmax(a.pgmin, pg);
+                EE = pg / (gam - 1.0) + 0.5 * (rho * vv2 + BB2);
+                irho = 1.0 / rho;
+            }
+            const double HH = (EE + pg) * irho;
+            sP[0 * NLC + t] = rho; sP[1 * NLC + t] = vx; sP[2 * NLC + t] = vy; sP[3 * NLC + t] = vz;
+            sP[4 * NLC + t] = Bx; sP[5 * NLC + t] = By; sP[6 * NLC + t] = Bz; sP[7 * NLC + t] = pg;
+            sP[8 * NLC + t] = HH;
+            // eigenst centre (src/ssprk.cpp:561-593), with DD, EE the floored values
+            const double pt = pg + 0.5 * BB2;
+            const double vdB = vx * Bx + vy * By + vz * Bz;
+            const double bbn2 = BB2 * irho;
+            const double bnx2 = Bx * Bx * irho;
+            const double cs2 = fmax(0.0, gam * fabs(pg * irho));
+            const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
+            const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
+            const double la = sqrt(fmax(0.0, bnx2));
+            const double ls = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 - root)));
+            sA[0 * NLC + t] = R(vx - lf); sA[1 * NLC + t] = R(vx - la); sA[2 * NLC + t] = R(vx - ls);
+            sA[3 * NLC + t] = R(vx);      sA[4 * NLC + t] = R(vx + ls); sA[5 * NLC + t] = R(vx + la);
+            sA[6 * NLC + t] = R(vx + lf);
+            double* U = sUst + t * 14;
+            double* Fc = sFc + t * 7;
+            Fc[0] = U[0] = rho * vx;                 // DD (floored) * vx
+            Fc[1] = U[1] = Mx * vx + pt - Bx * Bx;
+            Fc[2] = U[2] = My * vx - Bx * By;
+            Fc[3] = U[3] = Mz * vx - Bx * Bz;
+            Fc[4] = U[4] = By * vx - Bx * vy;
+            Fc[5] = U[5] = Bz * vx - Bx * vz;
+            Fc[6] = U[6] = (EE + pt) * vx - Bx * vdB;
+            U[7] = rho; U[8] = Mx; U[9] = My; U[10] = Mz; U[11] = By; U[12] = Bz; U[13] = EE;
+        }
+        __syncthreads();
+        mark(1);
+
+        // ------------------------------------------------------------ P1b
+        // cell differences of (F, q_proj) along each line, formed in FP64 and
+        // stored in the working type; shared by all 7 fields
+        for (int t = tid; t < NLC * 14; t += blockDim.x) {
+            const int c = (t / 14) % C;
+            sD[t] = (c + 1 < C) ? R(sUst[t + 14] - sUst[t]) : R(0);
+        }
+        __syncthreads();
+
+        // ------------------------------------------------------------ PR
+        // routing: features of every interface, the hard guard, the network
+        // (MODE 1), and the compacted list of interfaces that get full WENO
+        int nfull = NLF;
+        if constexpr (MODE != 0) {
+            if (tid < 2) s_cnt[tid] = 0u;
+            for (int t = tid; t < TL::NRp; t += blockDim.x) {
+                if (t >= NLF) {
+                    if constexpr (MODE == 1) {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) sX[t][k] = __float2bfloat16_rn(0.0f);
+                        sList[t] = 1;   // padding row: its logit is never read
+                    }
+                    continue;
+                }
+                const int l = t / F, f = t % F;
+                StencilCell sc[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const int c = l * C + f + k;
+                    const double vx = sP[1 * NLC + c], vy = sP[2 * NLC + c], vz = sP[3 * NLC + c];
+                    const double Bx = sP[4 * NLC + c], By = sP[5 * NLC + c], Bz = sP[6 * NLC + c];
+                    sc[k].rho = (float)sP[0 * NLC + c];
+                    sc[k].p = (float)sP[7 * NLC + c];
+                    sc[k].bmag = (float)sqrt(Bx * Bx + By * By + Bz * Bz);
+                    sc[k].vmag = (float)sqrt(vx * vx + vy * vy + vz * vz);
+                    sc[k].cf = (float)(sA[6 * NLC + c] - sA[3 * NLC + c]);
+                }
+                const int iface = c0 + f;
+                float prior = 1.0f;
+                if (line_ok(l) && iface <= n) prior = (float)a.route_prev[line_off(l) + (long long)(iface + 2) * sstride];
+                float ft[kRouterNF];
+                const bool guard = router_features(sc, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump,
+                                                   a.guard_floor, ft);
+                if constexpr (MODE == 1) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) sX[t][k] = __float2bfloat16_rn(k < kRouterNF ? ft[k] : 0.0f);
+                    // flat code (scratch in sList until compaction): 0 not flat, 1 + prior
+                    const bool flat = ft[0] == flat_feature && ft[1] == flat_feature && ft[2] == flat_feature &&
+                                      ft[3] == flat_feature && ft[4] == flat_feature;
+                    sList[t] = flat ? 1 + (prior > 0.5f ? 1 : 0) : 0;
+                }
+                if constexpr (MODE == 3) {
+#pragma unroll
+                    for (int k = 0; k < kRouterNF; ++k) sFt[t * 6 + k] = ft[k];
+                    sDev[t] = 0.0f;
+                }
+                sDec[t] = MODE == 3 ? 1 : (guard ? 1 : 0);
+            }
+            __syncthreads();
+            if constexpr (MODE == 1) {
+                const int w = tid >> 5, nw = blockDim.x >> 5;
+                const int lane = tid & 31;
+                for (int mt = w; mt < TL::NRp / 16; mt += nw) {
+                    const int code = lane < 16 ? sList[16 * mt + lane] : 1;
+                    if (__all_sync(0xffffffffu, code != 0)) {
+                        if (lane < 16) sLogit[16 * mt + lane] = s_flat_logit[code - 1];
+                    } else {
+                        router_mma_16rows(sRS, sX + 16 * mt, sLogit + 16 * mt);
+                    }
+                }
+                __syncthreads();
+                for (int t = tid; t < NLF; t += blockDim.x)
+                    if (sLogit[t] > a.route_thr) sDec[t] = 1;
+                __syncthreads();
+            }
+            if constexpr (ROUTED) {
+                if (tid < 32) {   // compaction by one warp
+                    int base = 0;
+                    for (int c0w = 0; c0w < NLF; c0w += 32) {
+                        const int t = c0w + tid;
+                        const bool full = t < NLF && sDec[t] != 0;
+                        const unsigned int m = __ballot_sync(0xffffffffu, full);
+                        if (full) sList[base + __popc(m & ((1u << tid) - 1u))] = t;
+                        base += __popc(m);
+                    }
+                    if (tid == 0) s_nfull = base;
+                }
+                __syncthreads();
+                nfull = s_nfull;
+            }
+        }
+
+        // ------------------------------------------------------------ P2a
+        for (int k = tid; k < nfull; k += blockDim.x) {
+            const int t = ROUTED ? sList[k] : k;
+            const int l = t / F, f = t % F;
+            const int c = l * C + f + 2;
+            const R rho = R(0.5 * (sP[0 * NLC + c] + sP[0 * NLC + c + 1]));
+            const R vx = R(0.5 * (sP[1 * NLC + c] + sP[1 * NLC + c + 1]));
+            const R vy = R(0.5 * (sP[2 * NLC + c] + sP[2 * NLC + c + 1]));
+            const R vz = R(0.5 * (sP[3 * NLC + c] + sP[3 * NLC + c + 1]));
+            const R Bx = R(0.5 * (sP[4 * NLC + c] + sP[4 * NLC + c + 1]));
+            const R By = R(0.5 * (sP[5 * NLC + c] + sP[5 * NLC + c + 1]));
+            const R Bz = R(0.5 * (sP[6 * NLC + c] + sP[6 * NLC + c + 1]));
+            const R HH = R(0.5 * (sP[8 * NLC + c] + sP[8 * NLC + c + 1]));
+            const R vv2 = vx * vx + vy * vy + vz * vz;
+            const R BB2 = Bx * Bx + By * By + Bz * Bz;
+            const R isqr = Math<R>::rsq(rho);
+            const R irho = isqr * isqr;
+            const R bbn2 = BB2 * irho;
+            const R bnx2 = Bx * Bx * irho;
+            const R cs2 = (gamR - R(1)) * (HH - R(0.5) * (vv2 + bbn2));
+            const R cs = Math<R>::sq(fmax(R(0), cs2));
+            const R root = Math<R>::sq(fmax(R(0), (bbn2 + cs2) * (bbn2 + cs2) - R(4) * bnx2 * cs2));
+            const R lf = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 + root)));
+            const R la = fabs(Bx) * isqr;
+            const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
+            const R Bt2 = By * By + Bz * Bz;
+            R bty, btz;
+            if (Bt2 >= R(1.0e-30)) { const R ib = Math<R>::rsq(Bt2); bty = By * ib; btz = Bz * ib; }
+            else { bty = R(0.70710678118654752440); btz = R(0.70710678118654752440); }
+            R af, as;
+            const R df = lf * lf - ls * ls;
+            if (df >= R(1.0e-30)) {
+                const R idf = Math<R>::rsq(df);
+                af = Math<R>::sq(fmax(R(0), cs2 - ls * ls)) * idf;
+                as = Math<R>::sq(fmax(R(0), lf * lf - cs2)) * idf;
+            } else { af = R(1); as = R(1); }
+            R* S = sS + t;
+            S[S_VX * NI] = vx; S[S_VY * NI] = vy; S[S_VZ * NI] = vz;
+            S[S_BY * NI] = By; S[S_BZ * NI] = Bz; S[S_VV2 * NI] = vv2;
+            S[S_CS * NI] = cs; S[S_CS2 * NI] = cs2; S[S_LF * NI] = lf; S[S_LS * NI] = ls;
+            S[S_AF * NI] = af; S[S_AS * NI] = as; S[S_BTY * NI] = bty; S[S_BTZ * NI] = btz;
+            S[S_SGNBX * NI] = sign1(Bx);
+            S[S_SQR * NI] = rho * isqr; S[S_ISQR * NI] = isqr;
+            S[S_SGNBT * NI] = (By != R(0)) ? sign1(By) : sign1(Bz);
+            S[S_FLIP * NI] = (cs >= la) ? R(1) : R(0);
+            S[S_BTV * NI] = bty * vy + btz * vz;
+            S[S_ICS2 * NI] = Math<R>::rcp(cs2);
+        }
+        __syncthreads();
+        mark(2);
+
+        // ------------------------------------------------------------ P2b
+        for (int t = tid; t < 7 * nfull; t += blockDim.x) {
+            const int r = t / nfull, k = t % nfull;
+            const int i = ROUTED ? sList[k] : k;
+            const R* S = sS + i;
+            const R vx = S[S_VX * NI], vy = S[S_VY * NI], vz = S[S_VZ * NI];
+            const R By = S[S_BY * NI], Bz = S[S_BZ * NI], vv2 = S[S_VV2 * NI];
+            const R cs = S[S_CS * NI], cs2 = S[S_CS2 * NI];
+            const R lf = S[S_LF * NI], ls = S[S_LS * NI], af = S[S_AF * NI], as = S[S_AS * NI];
+            const R bty = S[S_BTY * NI], btz = S[S_BTZ * NI], sgnBx = S[S_SGNBX * NI];
+            const R sqrtrho = S[S_SQR * NI], isqr = S[S_ISQR * NI], sgnBt = S[S_SGNBT * NI];
+            const bool flip24 = S[S_FLIP * NI] != R(0);
+            const R btv = S[S_BTV * NI], ics2 = S[S_ICS2 * NI];
+            R L[7], Rv[7];
+            switch (r) {
+                case 0: {
+                    L[0] = af * (gam1 * vv2 + lf * vx) - as * ls * btv * sgnBx;
+                    L[1] = af * (gam0 * vx - lf);
+                    L[2] = gam0 * af * vy + as * ls * bty * sgnBx;
+                    L[3] = gam0 * af * vz + as * ls * btz * sgnBx;
+                    L[4] = gam0 * af * By + cs * as * bty * sqrtrho;
+                    L[5] = gam0 * af * Bz + cs * as * btz * sqrtrho;
+                    L[6] = -gam0 * af;
+                    const R s = R(0.5) * ics2;
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) L[m] *= s;
+                    Rv[0] = af; Rv[1] = af * (vx - lf);
+                    Rv[2] = af * vy + as * ls * bty * sgnBx; Rv[3] = af * vz + as * ls * btz * sgnBx;
+                    Rv[4] = cs * as * bty * isqr; Rv[5] = cs * as * btz * isqr;
+                    Rv[6] = af * (lf * lf - lf * vx + R(0.5) * vv2 - gam2 * cs2) + as * ls * btv * sgnBx;
+                    break;
+                }
+                case 1: {
+                    L[0] = R(0.5) * (btz * vy - bty * vz); L[1] = R(0); L[2] = R(-0.5) * btz; L[3] = R(0.5) * bty;
+                    L[4] = R(0.5) * (-btz * sgnBx * sqrtrho); L[5] = R(0.5) * (bty * sgnBx * sqrtrho); L[6] = R(0);
+                    Rv[0] = R(0); Rv[1] = R(0); Rv[2] = -btz; Rv[3] = bty;
+                    Rv[4] = -btz * sgnBx * isqr; Rv[5] = bty * sgnBx * isqr; Rv[6] = bty * vz - btz * vy;
+                    break;
+                }
+                case 2: {
+                    L[0] = as * (gam1 * vv2 + ls * vx) + af * lf * btv * sgnBx;
+                    L[1] = gam0 * as * vx - as * ls;
+                    L[2] = gam0 * as * vy - af * lf * bty * sgnBx;
+                    L[3] = gam0 * as * vz - af * lf * btz * sgnBx;
+                    L[4] = gam0 * as * By - cs * af * bty * sqrtrho;
+                    L[5] = gam0 * as * Bz - cs * af * btz * sqrtrho;
+                    L[6] = -gam0 * as;
+                    const R s = R(0.5) * ics2;
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) L[m] *= s;
+                    Rv[0] = as; Rv[1] = as * (vx - ls);
+                    Rv[2] = as * vy - af * lf * bty * sgnBx; Rv[3] = as * vz - af * lf * btz * sgnBx;
+                    Rv[4] = -cs * af * bty * isqr; Rv[5] = -cs * af * btz * isqr;
+                    Rv[6] = as * (ls * ls - ls * vx + R(0.5) * vv2 - gam2 * cs2) - af * lf * btv * sgnBx;
+                    break;
+                }
+                case 3: {
+                    const R s = -gam0 * ics2;
+                    L[0] = (-cs2 / gam0 - R(0.5) * vv2) * s; L[1] = vx * s; L[2] = vy * s; L[3] = vz * s;
+                    L[4] = By * s; L[5] = Bz * s; L[6] = -s;
+                    Rv[0] = R(1); Rv[1] = vx; Rv[2] = vy; Rv[3] = vz; Rv[4] = R(0); Rv[5] = R(0); Rv[6] = R(0.5) * vv2;
+                    break;
+                }
+                case 4: {
+                    L[0] = as * (gam1 * vv2 - ls * vx) - af * lf * btv * sgnBx;
+                    L[1] = as * (gam0 * vx + ls);
+                    L[2] = gam0 * as * vy + af * lf * bty * sgnBx;
+                    L[3] = gam0 * as * vz + af * lf * btz * sgnBx;
+                    L[4] = gam0 * as * By - cs * af * bty * sqrtrho;
+                    L[5] = gam0 * as * Bz - cs * af * btz * sqrtrho;
+                    L[6] = -gam0 * as;
+                    const R s = R(0.5) * ics2;
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) L[m] *= s;
+                    Rv[0] = as; Rv[1] = as * (vx + ls);
+                    Rv[2] = as * vy + af * lf * bty * sgnBx; Rv[3] = as * vz + af * lf * btz * sgnBx;
+                    Rv[4] = -cs * af * bty * isqr; Rv[5] = -cs * af * btz * isqr;
+                    Rv[6] = as * (ls * ls + ls * vx + R(0.5) * vv2 - gam2 * cs2) + af * lf * btv * sgnBx;
+                    break;
+                }
+                case 5: {
+                    L[0] = R(0.5) * (btz * vy - bty * vz); L[1] = R(0); L[2] = R(-0.5) * btz; L[3] = R(0.5) * bty;
+                    L[4] = R(0.5) * (btz * sgnBx * sqrtrho); L[5] = R(0.5) * (-bty * sgnBx * sqrtrho); L[6] = R(0);
+                    Rv[0] = R(0); Rv[1] = R(0); Rv[2] = -btz; Rv[3] = bty;
+                    Rv[4] = btz * sgnBx * isqr; Rv[5] = -bty * sgnBx * isqr; Rv[6] = bty * vz - btz * vy;
+                    break;
+                }
+                default: {
+                    L[0] = af * (gam1 * vv2 - lf * vx) + as * ls * btv * sgnBx;
+                    L[1] = af * (gam0 * vx + lf);
+                    L[2] = gam0 * af * vy - as * ls * bty * sgnBx;
+                    L[3] = gam0 * af * vz - as * ls * btz * sgnBx;
+                    L[4] = gam0 * af * By + cs * as * bty * sqrtrho;
+                    L[5] = gam0 * af * Bz + cs * as * btz * sqrtrho;
+                    L[6] = -gam0 * af;
+                    const R s = R(0.5) * ics2;
+#pragma unroll
+                    for (int m = 0; m < 7; ++m) L[m] *= s;
+                    Rv[0] = af; Rv[1] = af * (vx + lf);
+                    Rv[2] = af * vy - as * ls * bty * sgnBx; Rv[3] = af * vz - as * ls * btz * sgnBx;
+                    Rv[4] = cs * as * bty * isqr; Rv[5] = cs * as * btz * isqr;
+                    Rv[6] = af * (lf * lf + lf * vx + R(0.5) * vv2 - gam2 * cs2) - as * ls * btv * sgnBx;
+                    break;
+                }
+            }
+            // sign convention (src/ssprk.cpp:789-818) as one factor per row/column
+            const bool flip = flip24 ? (r == 2 || r == 4) : (r == 0 || r == 6);
+            const R sg = flip ? sgnBt : R(1);
+            R* lo = sL + r * 7 * NI + i;
+            R* ro = sR + r * 7 * NI + i;
+#pragma unroll
+            for (int m = 0; m < 7; ++m) { lo[m * NI] = L[m] * sg; ro[m * NI] = Rv[m] * sg; }
+        }
+        __syncthreads();
+        mark(3);
+
+        // ------------------------------------------------------------ P3
+        if constexpr (!ROUTED) {
+            for (int t = tid; t < 7 * NL * NP; t += blockDim.x) {
+                const int m = t % 7, pr = t / 7;
+                const int l = pr / NP, p = pr % NP;
+                const int f0 = 2 * p;
+                const bool has1 = f0 + 1 < F;
+                const int i0 = l * F + f0;
+                const int i1 = has1 ? i0 + 1 : i0;
+                R L0[7], L1[7];
+#pragma unroll
+                for (int v = 0; v < 7; ++v) {
+                    L0[v] = sL[(m * 7 + v) * NI + i0];
+                    L1[v] = sL[(m * 7 + v) * NI + i1];
+                }
+                // interface f0 uses differences at cells f0..f0+4, f0+1 uses f0+1..f0+5
+                R dF0[5], dq0[5], dF1[5], dq1[5];
+                R amx0 = fabs(sA[m * NLC + l * C + f0]);
+                R amx1 = fabs(sA[m * NLC + l * C + (f0 + 1 < C ? f0 + 1 : C - 1)]);
+#pragma unroll
+                for (int cc = 0; cc < 6; ++cc) {
+                    int c = f0 + cc;
+                    c = c < C - 1 ? c : C - 2;
+                    const V2* u = reinterpret_cast<const V2*>(sD + (l * C + c) * 14);
+                    R D[14];
+#pragma unroll
+                    for (int h = 0; h < 7; ++h) { const V2 x = u[h]; D[2 * h] = x.x; D[2 * h + 1] = x.y; }
+                    const R av = fabs(sA[m * NLC + l * C + (c + 1)]);
+                    if (cc <= 4) {
+                        R pf = L0[0] * D[0], pq = L0[0] * D[7];
+#pragma unroll
+                        for (int v = 1; v < 7; ++v) { pf += L0[v] * D[v]; pq += L0[v] * D[7 + v]; }
+                        dF0[cc] = pf; dq0[cc] = pq;
+                        amx0 = fmax(amx0, av);
+                    }
+                    if (cc >= 1) {
+                        R pf = L1[0] * D[0], pq = L1[0] * D[7];
+#pragma unroll
+                        for (int v = 1; v < 7; ++v) { pf += L1[v] * D[v]; pq += L1[v] * D[7 + v]; }
+                        dF1[cc - 1] = pf; dq1[cc - 1] = pq;
+                        amx1 = fmax(amx1, av);
+                    }
+                }
+                if constexpr (MODE == 3) {
+                    R d0, d1;
+                    sFs[m * NI + i0] = weno_flux_d<R, true>(dF0, dq0, amx0, &d0);
+                    atomicMax(reinterpret_cast<int*>(&sDev[i0]), __float_as_int((float)d0));
+                    if (has1) {
+                        sFs[m * NI + i1] = weno_flux_d<R, true>(dF1, dq1, amx1, &d1);
+                        atomicMax(reinterpret_cast<int*>(&sDev[i1]), __float_as_int((float)d1));
+                    }
+                } else {
+                    sFs[m * NI + i0] = weno_flux_d<R>(dF0, dq0, amx0);
+                    if (has1) sFs[m * NI + i1] = weno_flux_d<R>(dF1, dq1, amx1);
+                }
+            }
+        } else {
+            // routed: pairs of entries of the compacted list, each with its own stencil
+            const int npair = (nfull + 1) / 2;
+            for (int t = tid; t < 7 * npair; t += blockDim.x) {
+                const int m = t % 7, p = t / 7;
+                const bool has1 = 2 * p + 1 < nfull;
+                const int i0 = sList[2 * p];
+                const int i1 = has1 ? sList[2 * p + 1] : i0;
+#pragma unroll
+                for (int w = 0; w < 2; ++w) {
+                    const int ii = w == 0 ? i0 : i1;
+                    if (w == 1 && !has1) break;
+                    const int l = ii / F, f = ii % F;
+                    R L0[7];
+#pragma unroll
+                    for (int v = 0; v < 7; ++v) L0[v] = sL[(m * 7 + v) * NI + ii];
+                    R dF0[5], dq0[5];
+                    R amx0 = fabs(sA[m * NLC + l * C + f]);
+#pragma unroll
+                    for (int cc = 0; cc < 5; ++cc) {
+                        const int c = f + cc;
+                        const V2* u = reinterpret_cast<const V2*>(sD + (l * C + c) * 14);
+                        R D[14];
+#pragma unroll
+                        for (int h = 0; h < 7; ++h) { const V2 x = u[h]; D[2 * h] = x.x; D[2 * h + 1] = x.y; }
+                        R pf = L0[0] * D[0], pq = L0[0] * D[7];
+#pragma unroll
+                        for (int v = 1; v < 7; ++v) { pf += L0[v] * D[v]; pq += L0[v] * D[7 + v]; }
+                        dF0[cc] = pf; dq0[cc] = pq;
+                        amx0 = fmax(amx0, fabs(sA[m * NLC + l * C + c + 1]));
+                    }
+                    sFs[m * NI + ii] = weno_flux_d<R>(dF0, dq0, amx0);
+                }
+            }
+        }
+        __syncthreads();
+        mark(4);
+
+        // ------------------------------------------------------------ P4
+        // per (interface, flux component): full WENO -> F_i + sum_m R(r,m) F^_m
+        // (back-projection in m order, src/ssprk.cpp:941-943); routed-linear
+        // interfaces -> the component-wise linear flux.  Components 4 and 5
+        // also form the CT terms (src/ssprk.cpp:973-993).
+        for (int t = tid; t < 7 * NLF; t += blockDim.x) {
+            const int r = t / NLF, i = t % NLF;
+            const int l = i / F, f = i % F;
+            const int c = l * C + f + 2;          // left cell of the interface
+            const double F2 = sFc[c * 7 + r];     // physical flux of that cell (central part)
+            double dF;
+            bool full = true;
+            if constexpr (ROUTED) full = sDec[i] != 0;
+            if (full) {
+                R acc = R(0);
+#pragma unroll
+                for (int m = 0; m < 7; ++m) acc += sR[(m * 7 + r) * NI + i] * sFs[m * NI + i];
+                dF = (double)acc + F2;
+            } else {
+                R amx = R(0);
+                R dFk[5], dqk[5];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const int cc = l * C + f + k;
+                    amx = fmax(amx, fmax(fabs(sA[0 * NLC + cc]), fabs(sA[6 * NLC + cc])));
+                    if (k < 5) { dFk[k] = sD[cc * 14 + r]; dqk[k] = sD[cc * 14 + 7 + r]; }
+                }
+                dF = (double)linear_flux_d<R>(dFk, dqk, amx) + F2;
+            }
+            sdF[r * NI + i] = dF;
+            const int iface = c0 + f;   // global interface index, face at padded iface + 2
+            const bool valid = line_ok(l) && iface <= n;
+            if (valid && (r == 4 || r == 5)) {
+                // CT terms: mean of B_n v_t over the two cells
+                const int vt = r == 4 ? 2 : 3;
+                const double x1 = sP[4 * NLC + c] * sP[vt * NLC + c];
+                const double x2 = sP[4 * NLC + c + 1] * sP[vt * NLC + c + 1];
+                const long long o = line_off(l) + (long long)(iface + 2) * sstride;
+                double avg;
+                if (a.ct4) {
+                    // fourth-order midpoint value (-1, 9, 9, -1) / 16 over cells c-1 .. c+2
+                    const double x0 = sP[4 * NLC + c - 1] * sP[vt * NLC + c - 1];
+                    const double x3 = sP[4 * NLC + c + 2] * sP[vt * NLC + c + 2];
+                    avg = (-x0 + 9.0 * x1 + 9.0 * x2 - x3) / 16.0;
+                } else {
+                    // the reference's two-point form (-0, 9, 9, -0) / 18
+                    avg = (9.0 * x1 + 9.0 * x2) / 18.0;
+                }
+                (r == 4 ? a.cta : a.ctb)[o] = dF + avg;
+            }
+            if constexpr (MODE != 0) {
+                // a tile's last interface is also the next tile's first: the
+                // lower tile owns it unless it is the line's last face
+                if (valid && r == 0 && (f < T || iface == n)) {
+                    const long long o = line_off(l) + (long long)(iface + 2) * sstride;
+                    if constexpr (ROUTED) {
+                        a.route_next[o] = (unsigned char)(full ? 1 : 0);
+                        atomicAdd(&s_cnt[full ? 0 : 1], 1u);
+                    }
+                    if constexpr (MODE == 3) {
+                        a.route_next[o] = (unsigned char)(sDev[i] > 0.1f ? 1 : 0);
+                        // sampled tiles: a hash of the tile index, so the
+                        // sample does not alias with the tile grid
+                        const unsigned long long hs = (unsigned long long)tile * 0x9E3779B97F4A7C15ull;
+                        if ((unsigned int)(hs >> 32) % a.collect_every == 0u) {
+                            const unsigned int slot = atomicAdd(a.collect_n, 1u);
+                            if (slot < a.collect_cap) {
+                                float* rec = a.collect + 8ull * slot;
+#pragma unroll
+                                for (int k = 0; k < 6; ++k) rec[k] = sFt[i * 6 + k];
+                                rec[6] = sDev[i] > 0.1f ? 1.0f : 0.0f;
+                                rec[7] = sDev[i];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if constexpr (ROUTED) {
+            if (tid == 0) {
+                atomicAdd(&a.route_count[0], (unsigned long long)s_cnt[0]);
+                atomicAdd(&a.route_count[1], (unsigned long long)s_cnt[1]);
+            }
+        }
+        mark(5);
+
+        // ------------------------------------------------------------ P5
+        {
+            const bool ok = mbar_wait_bounded(&bars[2], (par_bits >> 2) & 1u, kWaitLimit);
+            if (__syncthreads_or(!ok)) { bail(); return; }
+        }
+        par_bits ^= 4u;
+        pend_bits &= ~4u;
+        const double dtdl = *a.dtdl;
+        for (int t = tid; t < 8 * NL * T; t += blockDim.x) {
+            int v, l, ct;
+            if (DIR == 0) { v = t / (NL * T); const int r = t % (NL * T); l = r / T; ct = r % T; }
+            else { v = t / (NL * T); const int r = t % (NL * T); ct = r / NL; l = r % NL; }
+            const int s = c0 + ct + 3;
+            if (!line_ok(l) || s > n + 2) continue;
+            const int rr = v < 4 ? v : v - 1;     // flux row of line variable v (v = 4: normal B)
+            const int fi = l * F + ct;
+            const double delta = (v == 4) ? 0.0 : -dtdl * (sdF[rr * NI + fi + 1] - sdF[rr * NI + fi]);
+            const int gv = perm_of(DIR, v);
+            const long long o = (long long)gv * g.fs + line_off(l) + (long long)s * sstride;
+            const double cur = oraw(gv, l, ct);   // q(iw) (accumulate) or the RK base
+            if (a.mode == 0) {
+                if (v != 4) a.qout[o] = cur + delta;
+            } else if (a.mode == 1) {
+                a.qout[o] = a.k1 * cur + a.k3 * qraw(v, l, ct + 3) + delta;
+            } else {
+                a.qout[o] = cur + delta;
+            }
+        }
+        __syncthreads();   // every read of the update operand / raw tile is done
+        {
+            const long long next = advance(tile + gridDim.x);
+            if (tid == 0 && next < ntiles) {
+                issued_ok = issue(next, 1, 0) && issued_ok;
+                pend_bits |= 4u;
+            }
+        }
+        mark(6);
+        buf ^= 1;
+    }   // tile loop
+}
+
+}  // namespace
+}  // namespace how

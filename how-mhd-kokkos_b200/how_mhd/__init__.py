@@ -50,6 +50,7 @@ class Params(ctypes.Structure):
         ("router", ctypes.c_int),
         ("seed", ctypes.c_uint64),
         ("problem_par", ctypes.c_double * 8),
+        ("ct_avg", ctypes.c_int),
     ]
 
     @property
@@ -69,6 +70,8 @@ def _load():
     D = ctypes.POINTER(ctypes.c_double)
     P = ctypes.POINTER(Params)
     V = ctypes.c_void_p
+    F = ctypes.POINTER(ctypes.c_float)
+    U64P = ctypes.POINTER(ctypes.c_ulonglong)
     sig = {
         "how_params_default": ([P], ctypes.c_int),
         "how_parse_input": ([ctypes.c_char_p, P], ctypes.c_int),
@@ -104,6 +107,30 @@ def _load():
         "how_get_kernel_timing": ([V, D, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
         "how_measure_fp64_peak": ([D, ctypes.c_int], ctypes.c_int),
         "how_sweep_phase_profile": ([V, ctypes.c_int, ctypes.c_double, D, ctypes.c_int], ctypes.c_int),
+        "how_ensemble_create": ([P, ctypes.c_int, ctypes.POINTER(V)], ctypes.c_int),
+        "how_ensemble_destroy": ([V], ctypes.c_int),
+        "how_ensemble_size": ([V], ctypes.c_int),
+        "how_ensemble_member": ([V, ctypes.c_int], V),
+        "how_ensemble_init": ([V], ctypes.c_int),
+        "how_ensemble_set_shapes": ([V, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "how_ensemble_get_shapes": ([V, ctypes.POINTER(ctypes.c_int), D], ctypes.c_int),
+        "how_ensemble_shape_info": ([ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "how_ensemble_run": ([V, ctypes.c_long, ctypes.POINTER(ctypes.c_long)], ctypes.c_int),
+        "how_ensemble_member_status": ([V, ctypes.c_int, D, ctypes.POINTER(ctypes.c_long),
+                                        ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "how_ensemble_graph_launches": ([V], ctypes.c_long),
+        "how_router_param_count": ([], ctypes.c_int),
+        "how_router_default": ([F, ctypes.c_int, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+        "how_router_set_weights": ([V, F, ctypes.c_int], ctypes.c_int),
+        "how_router_configure": ([V, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+        "how_router_stats": ([V, U64P, U64P, ctypes.c_int], ctypes.c_int),
+        "how_collect_begin": ([V, ctypes.c_uint, ctypes.c_uint], ctypes.c_int),
+        "how_collect_end": ([V, F, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)], ctypes.c_int),
+        "how_router_train": ([F, F, F, ctypes.c_long, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                              ctypes.c_ulonglong, F], ctypes.c_int),
+        "how_router_grad": ([F, F, F, ctypes.c_long, ctypes.c_float, F, F], ctypes.c_int),
+        "how_router_infer": ([F, F, ctypes.c_long, F, F], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -123,6 +150,17 @@ def _check(rc):
 
 def _dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _f32(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
 
 
 def lib():
@@ -153,7 +191,8 @@ def make_parameters(**kw) -> Params:
     """Parameters from keywords using the input.in key names (bc as strings)."""
     lines = []
     for k, v in kw.items():
-        lines.append(f"{k} {v!r}" if isinstance(v, float) else f"{k} {v}")
+        # repr of a float round-trips exactly (numpy scalars as plain floats)
+        lines.append(f"{k} {float(v)!r}" if isinstance(v, float) else f"{k} {v}")
     return read_parameters("\n".join(lines) + "\n")
 
 
@@ -204,7 +243,22 @@ class Domain:
         self.params = p
         self.shape = p.shape
 
+    @classmethod
+    def _borrowed(cls, handle, owner):
+        """A view of a context owned by someone else (an ensemble member)."""
+        d = cls.__new__(cls)
+        d._h = ctypes.c_void_p(handle)
+        d._owner = owner
+        p = Params()
+        _check(_lib.how_get_params(d._h, ctypes.byref(p)))
+        d.params = p
+        d.shape = p.shape
+        return d
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.how_destroy(self._h)
             self._h = None
@@ -298,6 +352,34 @@ class Domain:
     def sync(self):
         _check(_lib.how_sync(self._h))
 
+    # ---- learned routing
+    def set_router(self, weights, mode="learned", threshold=0.0, guard_jump=0.25, guard_floor=100.0):
+        """Route interfaces between full characteristic WENO5 and the linear
+        flux.  mode: "off", "learned" (network + guard) or "guard" (guard only)."""
+        m = {"off": 0, "learned": 1, "guard": 2}[mode] if isinstance(mode, str) else int(mode)
+        if weights is not None:
+            w = _f32(weights, ROUTER_PARAMS)
+            _check(_lib.how_router_set_weights(self._h, _fptr(w), w.size))
+        _check(_lib.how_router_configure(self._h, m, threshold, guard_jump, guard_floor))
+
+    def router_stats(self, reset=False):
+        """(full, cheap) interface counts since the last reset."""
+        a, b = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+        _check(_lib.how_router_stats(self._h, ctypes.byref(a), ctypes.byref(b), int(reset)))
+        return a.value, b.value
+
+    def collect_begin(self, capacity, every=1):
+        _check(_lib.how_collect_begin(self._h, capacity, every))
+        self._collect_cap = capacity
+
+    def collect_end(self):
+        """Records (n, 8): 6 features, label, max weight departure."""
+        cap = getattr(self, "_collect_cap", 0)
+        out = np.zeros((max(cap, 1), 8), np.float32)
+        n = ctypes.c_uint(0)
+        _check(_lib.how_collect_end(self._h, _fptr(out), cap, ctypes.byref(n)))
+        return out[: n.value].copy()
+
     @property
     def kernel_launches(self) -> int:
         return _lib.how_kernel_launches(self._h)
@@ -309,6 +391,116 @@ class Domain:
     @property
     def device_bytes(self) -> int:
         return _lib.how_device_bytes(self._h)
+
+
+# ---------------------------------------------------------------- ensembles
+class Ensemble:
+    """A batched ensemble (how_ensemble): independent runs of uneven sizes
+    advanced together, one launch per kernel for all members, one CUDA graph
+    per step."""
+
+    def __init__(self, params_list):
+        arr = (Params * len(params_list))(*params_list)
+        h = ctypes.c_void_p()
+        _check(_lib.how_ensemble_create(arr, len(params_list), ctypes.byref(h)))
+        self._h = h
+        self.n = len(params_list)
+        self.members = [Domain._borrowed(_lib.how_ensemble_member(h, m), self) for m in range(self.n)]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            for d in self.members:
+                d._h = None
+            _lib.how_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def init(self):
+        _check(_lib.how_ensemble_init(self._h))
+
+    def set_shapes(self, sx, sy, sz=0):
+        _check(_lib.how_ensemble_set_shapes(self._h, sx, sy, sz))
+
+    def shapes(self):
+        """(chosen shape per direction, autotuner sweep ms [dir][candidate])"""
+        s = (ctypes.c_int * 3)()
+        ms = np.zeros(9)
+        _check(_lib.how_ensemble_get_shapes(self._h, s, _dptr(ms)))
+        return list(s), ms.reshape(3, 3)
+
+    @staticmethod
+    def shape_info(direction, shape):
+        a, b = ctypes.c_int(0), ctypes.c_int(0)
+        _check(_lib.how_ensemble_shape_info(direction, shape, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def run(self, max_steps=-1):
+        s = ctypes.c_long(0)
+        _check(_lib.how_ensemble_run(self._h, max_steps, ctypes.byref(s)))
+        return s.value
+
+    def status(self, m):
+        """(time, steps, done) of member m"""
+        t, s, d = ctypes.c_double(0), ctypes.c_long(0), ctypes.c_int(0)
+        _check(_lib.how_ensemble_member_status(self._h, m, ctypes.byref(t), ctypes.byref(s), ctypes.byref(d)))
+        return t.value, s.value, bool(d.value)
+
+    @property
+    def graph_launches(self):
+        return _lib.how_ensemble_graph_launches(self._h)
+
+
+# ------------------------------------------------------------ router training
+ROUTER_PARAMS = _lib.how_router_param_count()
+
+
+def default_router():
+    """(weights, logit threshold) built into the library (`router on`)."""
+    w = np.zeros(ROUTER_PARAMS, np.float32)
+    t = ctypes.c_float(0)
+    _check(_lib.how_router_default(_fptr(w), ROUTER_PARAMS, ctypes.byref(t)))
+    return w, float(t.value)
+
+
+def router_grad(w, feats, labels, pos_weight=1.0):
+    """GPU gradient (and loss) of the mean weighted BCE at w."""
+    w = _f32(w, ROUTER_PARAMS)
+    x = _f32(feats)
+    y = _f32(labels)
+    g = np.zeros(ROUTER_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    _check(_lib.how_router_grad(_fptr(w), _fptr(x), _fptr(y), y.size, pos_weight, _fptr(g), _fptr(loss)))
+    return g, float(loss[0])
+
+
+def router_train(w, feats, labels, iters, batch=4096, lr=3e-3, pos_weight=1.0, seed=1):
+    """Adam on the GPU; returns (weights, per-iteration loss)."""
+    w = _f32(w, ROUTER_PARAMS).copy()
+    x = _f32(feats)
+    y = _f32(labels)
+    hist = np.zeros(iters, np.float32)
+    _check(_lib.how_router_train(_fptr(w), _fptr(x), _fptr(y), y.size, pos_weight, iters, batch, lr, seed,
+                                 _fptr(hist)))
+    return w, hist
+
+
+def router_infer(w, feats):
+    """(FP32 logits, BF16 tensor-core logits) of feature rows."""
+    w = _f32(w, ROUTER_PARAMS)
+    x = _f32(feats)
+    n = x.size // 6
+    a = np.zeros(n, np.float32)
+    b = np.zeros(n, np.float32)
+    _check(_lib.how_router_infer(_fptr(w), _fptr(x), n, _fptr(a), _fptr(b)))
+    return a, b
 
 
 # reference-named free functions over a Domain

@@ -65,6 +65,9 @@ typedef struct how_params {
     int router;                /* 0 off, 1 learned WENO routing   (key: router off|on)        */
     uint64_t seed;             /* problem seed                    (key: seed)                 */
     double problem_par[8];     /* problem parameters              (keys: par0..par7)          */
+    int ct_avg;                /* points of the face average of B_n v_t in the CT flux terms:
+                                * 2 = the reference's (src/ssprk.cpp:976-989, default),
+                                * 4 = fourth-order (-1, 9, 9, -1)/16  (key: ct_avg 2|4)      */
 } how_params;
 
 typedef struct how_ctx how_ctx;
@@ -166,6 +169,62 @@ int how_get_kernel_timing(how_ctx* ctx, double* total_ms, long* launches);
  * out[0..6] = phases (load, primitives, differences+scalars, eigenvector
  * rows, projection+WENO, back-projection+CT, update); out[7] = blocks. */
 int how_sweep_phase_profile(how_ctx* ctx, int dir, double dt, double* out, int nout);
+/* ------------------------------------------------------ batched ensembles */
+/* No counterpart in the reference (which runs one domain per job).  Many
+ * independent runs (members, each with its own how_params: size, gamma,
+ * problem, boundaries, tend, nt) advance together: every kernel of a time step
+ * is launched once for all members (the sweeps as one persistent launch per
+ * direction over every member's tiles) and the step is captured in a CUDA
+ * graph that is replayed until each member has reached its tend.  A member
+ * computes exactly what how_run computes for it alone.  Members need nx > 1
+ * and run the plain FP64 method.  how_ensemble_member gives the member's
+ * context for state access (valid until how_ensemble_destroy, which also
+ * destroys the members). */
+typedef struct how_ensemble how_ensemble;
+int how_ensemble_create(const how_params* members, int n, how_ensemble** out);
+int how_ensemble_destroy(how_ensemble* e);
+int how_ensemble_size(const how_ensemble* e);
+how_ctx* how_ensemble_member(how_ensemble* e, int m);
+/* init_problem of every member; member times back to 0 */
+int how_ensemble_init(how_ensemble* e);
+/* Sweep tile shapes per direction (index into the candidate list of
+ * how_ensemble_shape_info).  Without this call the first how_ensemble_run
+ * autotunes: one real step per candidate, then the fastest per direction. */
+int how_ensemble_set_shapes(how_ensemble* e, int sx, int sy, int sz);
+int how_ensemble_get_shapes(const how_ensemble* e, int* shapes /*[3]*/, double* sweep_ms /*[3 x 3]*/);
+int how_ensemble_shape_info(int dir, int shape, int* lines, int* cells);
+/* Advance until every member reaches its tend (max_steps < 0) or for at most
+ * max_steps steps; *steps_out = the most steps any member has taken. */
+int how_ensemble_run(how_ensemble* e, long max_steps, long* steps_out);
+int how_ensemble_member_status(const how_ensemble* e, int m, double* time, long* steps, int* done);
+long how_ensemble_graph_launches(const how_ensemble* e);
+
+/* ------------------------------------------------------- learned routing */
+/* No counterpart in the reference (the north star's learned part).  A
+ * 6 -> 32 -> 32 -> 1 GELU network, packed FP32 as W1[32][6], b1[32],
+ * W2[32][32], b2[32], w3[32], b3 (how_router_param_count() floats), routes
+ * each interface of each sweep to the full characteristic WENO5 or to a
+ * component-wise linear-weight fifth-order flux; a hard jump/positivity guard
+ * forces full WENO.  Inference runs on the tensor cores (BF16, FP32
+ * accumulate) inside the sweep kernel. */
+int how_router_param_count(void);
+/* the built-in trained weights and logit threshold (what `router on` uses) */
+int how_router_default(float* w, int n, float* threshold);
+int how_router_set_weights(how_ctx* ctx, const float* w, int n);
+/* mode 0 off, 1 network + guard, 2 guard only; full WENO when logit > threshold */
+int how_router_configure(how_ctx* ctx, int mode, float threshold, float guard_jump, float guard_floor);
+int how_router_stats(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap, int reset);
+/* Label collection from the plain FP64 method (records of 8 floats). */
+int how_collect_begin(how_ctx* ctx, unsigned int capacity, unsigned int every);
+int how_collect_end(how_ctx* ctx, float* out, unsigned int cap, unsigned int* n);
+/* Hand-written GPU training (FP32, Adam) of w in place, its gradient, and
+ * batched inference by the FP32 network and by the BF16 tensor-core path. */
+int how_router_train(float* w, const float* feats, const float* labels, long n, float pos_weight, int iters,
+                     int batch, float lr, unsigned long long seed, float* loss_hist);
+int how_router_grad(const float* w, const float* feats, const float* labels, long n, float pos_weight,
+                    float* grad_out, float* loss_out);
+int how_router_infer(const float* w, const float* feats, long n, float* out_fp32, float* out_bf16);
+
 /* ---------------------------------------------------- allocation-free use */
 /* Capacity of the fixed scratch behind how_tstep_noalloc, in (i, j) lines. */
 #define HOW_NOALLOC_MAX_LINES 262144

@@ -30,6 +30,10 @@
 
 namespace {
 
+// 1: fourth-order face value of B_n v_t in the CT terms (an option of the
+// B200 path, ct_avg 4); 0: the reference's two-point form
+int g_ct_avg4 = 0;
+
 constexpr int NVAR = 8;
 
 // ------------------------------------------------------------ counting scalar
@@ -388,14 +392,23 @@ void sweep_line(double* qx, int n, const Prm& P, double dtdl, double* dq, double
     // CT terms (src/ssprk.cpp:973-993)
     for (int i = 0; i <= n; ++i) {
         const int im1 = i + 1, i0 = i + 2, ip1 = i + 3, ip2 = i + 4;
-        const double ftmp1 = (-0.0 * (ux[4 * Pn + im1] * ux[2 * Pn + im1])
-                              + 9.0 * (ux[4 * Pn + i0] * ux[2 * Pn + i0])
-                              + 9.0 * (ux[4 * Pn + ip1] * ux[2 * Pn + ip1])
-                              - 0.0 * (ux[4 * Pn + ip2] * ux[2 * Pn + ip2])) / 18.0;
-        const double ftmp2 = (-0.0 * (ux[4 * Pn + im1] * ux[3 * Pn + im1])
-                              + 9.0 * (ux[4 * Pn + i0] * ux[3 * Pn + i0])
-                              + 9.0 * (ux[4 * Pn + ip1] * ux[3 * Pn + ip1])
-                              - 0.0 * (ux[4 * Pn + ip2] * ux[3 * Pn + ip2])) / 18.0;
+        double ftmp1, ftmp2;
+        if (g_ct_avg4) {
+            // optional fourth-order face value (-1, 9, 9, -1) / 16 (not in the reference)
+            ftmp1 = (-(ux[4 * Pn + im1] * ux[2 * Pn + im1]) + 9.0 * (ux[4 * Pn + i0] * ux[2 * Pn + i0])
+                     + 9.0 * (ux[4 * Pn + ip1] * ux[2 * Pn + ip1]) - (ux[4 * Pn + ip2] * ux[2 * Pn + ip2])) / 16.0;
+            ftmp2 = (-(ux[4 * Pn + im1] * ux[3 * Pn + im1]) + 9.0 * (ux[4 * Pn + i0] * ux[3 * Pn + i0])
+                     + 9.0 * (ux[4 * Pn + ip1] * ux[3 * Pn + ip1]) - (ux[4 * Pn + ip2] * ux[3 * Pn + ip2])) / 16.0;
+        } else {
+            ftmp1 = (-0.0 * (ux[4 * Pn + im1] * ux[2 * Pn + im1])
+                     + 9.0 * (ux[4 * Pn + i0] * ux[2 * Pn + i0])
+                     + 9.0 * (ux[4 * Pn + ip1] * ux[2 * Pn + ip1])
+                     - 0.0 * (ux[4 * Pn + ip2] * ux[2 * Pn + ip2])) / 18.0;
+            ftmp2 = (-0.0 * (ux[4 * Pn + im1] * ux[3 * Pn + im1])
+                     + 9.0 * (ux[4 * Pn + i0] * ux[3 * Pn + i0])
+                     + 9.0 * (ux[4 * Pn + ip1] * ux[3 * Pn + ip1])
+                     - 0.0 * (ux[4 * Pn + ip2] * ux[3 * Pn + ip2])) / 18.0;
+        }
         bsy[i] = dF[4 * (n + 1) + i] + ftmp1;
         bsz[i] = dF[5 * (n + 1) + i] + ftmp2;
     }
@@ -834,6 +847,7 @@ extern "C" {
 void* oracle_create(const oracle_params* p) { return new Oracle(*p); }
 void oracle_destroy(void* h) { delete static_cast<Oracle*>(h); }
 void oracle_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
+void oracle_set_ct_avg(int points) { g_ct_avg4 = points == 4 ? 1 : 0; }
 
 int oracle_init_problem(void* h, const char* name) {
     return init_problem(*static_cast<Oracle*>(h), std::string(name));

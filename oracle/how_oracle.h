@@ -41,6 +41,7 @@ int    oracle_run(void* h, double tend, int nt, long max_steps,
  * ct_a/ct_b receive the two CT flux arrays that sweep fills. */
 void   oracle_sweep(void* h, int dir, double dt, double* q1_out, double* ct_a, double* ct_b);
 void   oracle_set_threads(int n);
+void   oracle_set_ct_avg(int points);   /* 2 (reference) or 4 */
 /* algorithmic FP64 operation counts (add/sub/mul/div/sqrt/max/abs as 1) of the
  * per-cell and per-interface kernels, from a counting scalar type. */
 void   oracle_flop_counts(double* out, int cap);

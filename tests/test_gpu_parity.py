@@ -173,3 +173,29 @@ def test_single_sweep(direction):
         r = ref[tuple(sl)]
         e = np.abs(g - r).sum() / max(np.abs(r).sum(), 1e-300)
         assert e <= TOL_Q, f"sweep {direction} CT array {w}: {e}"
+
+
+def test_ct_avg4_vs_oracle():
+    """The optional fourth-order CT face average (ct_avg 4) against the
+    oracle run with the same option, 10 steps of the 3-D smooth wave."""
+    from howtest import oracle_lib
+    hm, p, dom, o = _setup("alfven3d", (24, 24, 24), ("periodic",) * 3, 5.0 / 3.0, ct_avg=4)
+    lib = oracle_lib()
+    lib.oracle_set_ct_avg(4)
+    try:
+        q0 = hm.problem_state(p)
+        o.set_state(q0)
+        rc, t_o, dts_o = o.run(1.0, max_steps=10)
+        qo = o.get_q(0)
+    finally:
+        lib.oracle_set_ct_avg(2)
+    with dom:
+        dom.init_problem()
+        t, s, dts = dom.run(0.0, 10, dts_cap=10)
+        q = dom.get_state(0)
+    np.testing.assert_allclose(dts, dts_o, rtol=1e-13)
+    a, b = active(q, 24, 24, 24), active(qo, 24, 24, 24)
+    for v in range(8):
+        sc = np.abs(b[v]).sum()
+        if sc > 0:
+            assert np.abs(a[v] - b[v]).sum() <= 1e-12 * sc, v

@@ -1,0 +1,151 @@
+"""Learned WENO router: the BF16 tensor-core inference and the FP32 training
+kernels against the CPU restatement in router_ref.py, label collection from
+the plain solver, and the routed sweep at its two limits (every interface to
+full WENO reproduces the plain method; every interface to the linear flux is
+a stable fifth-order scheme)."""
+import numpy as np
+import pytest
+
+import router_ref as rr
+from howtest import active
+
+pytestmark = pytest.mark.gpu
+
+
+def _feats(n, seed=0):
+    rng = np.random.default_rng(seed)
+    x = np.empty((n, 6), np.float32)
+    x[:, :5] = rng.uniform(-6.0, 0.5, (n, 5))
+    x[:, 5] = rng.integers(0, 2, n)
+    return x
+
+
+@pytest.mark.parametrize("n", [16, 1000, 4101])
+def test_router_inference_fp32_and_bf16(n):
+    import how_mhd as hm
+    w = rr.init_weights(3)
+    x = _feats(n, 1)
+    lf, lb = hm.router_infer(w, x)
+    ref = rr.forward(w, x)
+    scale = max(1.0, np.abs(ref).max())
+    assert np.abs(lf - ref).max() <= 1e-5 * scale
+    refb = rr.forward_bf16(w, x)
+    # same BF16 operands; FP32 sums in another order and tanhf vs tanh
+    assert np.abs(lb - refb).max() <= 2e-3 * scale, np.abs(lb - refb).max()
+    # and BF16 stays close to the FP32 network
+    assert np.abs(lb - ref).max() <= 0.1 * scale
+
+
+def test_router_gradient_vs_cpu():
+    import how_mhd as hm
+    w = rr.init_weights(5)
+    x = _feats(3000, 2)
+    y = (np.random.default_rng(3).random(3000) < 0.25).astype(np.float32)
+    g, loss = hm.router_grad(w, x, y, pos_weight=3.0)
+    lref, gref = rr.loss_and_grad(w, x, y, 3.0)
+    assert abs(loss - lref) <= 1e-5 * abs(lref)
+    err = np.abs(g - gref).max() / np.abs(gref).max()
+    assert err <= 1e-4, err
+    idx = [0, 50, 191, 192, 223, 224, 700, 1247, 1248, 1279, 1280, 1311, 1312]
+    fd = rr.fd_grad(w, x, y, idx, 3.0)
+    np.testing.assert_allclose(g[idx], fd, rtol=2e-3, atol=1e-4 * np.abs(gref).max())
+
+
+def test_router_training_learns_a_boundary():
+    import how_mhd as hm
+    x = _feats(20000, 4)
+    y = ((x[:, 0] > -2.0) | (x[:, 1] > -1.5)).astype(np.float32)
+    w0 = rr.init_weights(7)
+    w, hist = hm.router_train(w0, x, y, iters=600, batch=2048, lr=3e-3, pos_weight=1.0, seed=11)
+    assert hist[-50:].mean() < 0.5 * hist[:10].mean()
+    acc = ((rr.forward(w, x) > 0) == (y > 0.5)).mean()
+    assert acc > 0.97, acc
+    # deterministic: same seed, same weights
+    w2, _ = hm.router_train(w0, x, y, iters=600, batch=2048, lr=3e-3, pos_weight=1.0, seed=11)
+    np.testing.assert_array_equal(w, w2)
+
+
+def _domain(prob, n, tend=100.0, **kw):
+    import how_mhd as hm
+    p = hm.make_parameters(nx=n[0], ny=n[1], nz=n[2], nt=1, tend=tend, gam=5.0 / 3.0, cour=0.4,
+                           problem=prob, **kw)
+    return hm.Domain(p)
+
+
+def test_collect_labels_from_plain_solver():
+    with _domain("orszag_tang", (64, 64, 1)) as d:
+        d.init_problem()
+        d.run(0.0, 20)
+        ref = d.get_state(0)
+        d.collect_begin(1 << 20, every=1)
+        d.run(0.0, 2)
+        rec = d.collect_end()
+    # 2 steps x 5 stages x 2 directions x 65 faces x 64 lines: every active
+    # face once (a face shared by two tiles is recorded by one)
+    assert len(rec) == 2 * 5 * 2 * 65 * 64
+    assert np.isfinite(rec).all()
+    assert set(np.unique(rec[:, 6])) == {0.0, 1.0}
+    assert ((rec[:, 6] > 0.5) == (rec[:, 7] > 0.1)).all()
+    assert set(np.unique(rec[:, 5])) <= {0.0, 1.0}
+    assert np.isfinite(ref).all()
+
+
+def test_collect_matches_plain_run():
+    """Collection runs the plain FP64 method: the state is unchanged by it."""
+    with _domain("orszag_tang", (64, 64, 1)) as d:
+        d.init_problem()
+        d.run(0.0, 5)
+        a = d.get_state(0)
+    with _domain("orszag_tang", (64, 64, 1)) as d:
+        d.init_problem()
+        d.collect_begin(1 << 16, every=3)
+        d.run(0.0, 5)
+        d.collect_end()
+        b = d.get_state(0)
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("prob,n,kw", [
+    ("orszag_tang", (128, 128, 1), {}),
+    ("blast3d_b", (32, 32, 32), dict(rhomin=1e-6, pgmin=1e-6)),
+])
+def test_routed_all_full_equals_plain(prob, n, kw):
+    with _domain(prob, n, **kw) as d:
+        d.init_problem()
+        d.run(0.0, 8)
+        a = d.get_state(0)
+    with _domain(prob, n, **kw) as d:
+        d.init_problem()
+        d.set_router(rr.init_weights(0), "learned", threshold=-1e30)
+        d.run(0.0, 8)
+        b = d.get_state(0)
+        full, cheap = d.router_stats()
+    assert cheap == 0 and full > 0
+    aa, bb = active(a, *n), active(b, *n)
+    for v in range(8):
+        s = np.abs(aa[v]).sum()
+        if s > 0:
+            assert np.abs(bb[v] - aa[v]).sum() <= 1e-13 * s, v
+
+
+def test_routed_all_linear_converges_to_plain_on_alfven():
+    """Every interface on the linear flux (guard off) on the smooth 1-D
+    Alfven wave, one period: the difference from the full method is the gap
+    between two fifth-order dissipations, so it shrinks by >= 2^4 per
+    refinement."""
+    diffs = []
+    for n in (32, 64):
+        out = []
+        for routed in (False, True):
+            with _domain("alfven3d", (n, 1, 1), tend=1.0) as d:
+                d.init_problem()
+                if routed:
+                    d.set_router(rr.init_weights(0), "learned", threshold=1e30, guard_jump=1e30, guard_floor=0.0)
+                d.run(0.0, 10 ** 6)
+                if routed:
+                    full, cheap = d.router_stats()
+                    assert full == 0 and cheap > 0
+                out.append(active(d.get_state(0), n, 1, 1))
+        assert np.isfinite(out[1]).all()
+        diffs.append(np.abs(out[1][5] - out[0][5]).mean())
+    assert diffs[1] > 0 and diffs[0] / diffs[1] >= 16.0, diffs

@@ -12,7 +12,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from howtest import GOLDEN, REF_BIN, CPUOracle, active, read_dump, run_ref, write_dump, write_input
+from howtest import GOLDEN, REF_BIN, CPUOracle, active, oracle_lib, read_dump, run_ref, write_dump, write_input
 
 FIXTURES = sorted(GOLDEN.glob("*.npz"))
 
@@ -104,3 +104,31 @@ def test_reference_dump_stages_equals_reference_ssprk(tmp_path):
     a = run_ref(inp, tmp_path / "a.bin", "--dump-stages")
     b = run_ref(inp, tmp_path / "b.bin", "--steps", 1)
     np.testing.assert_array_equal(active(a["final_q"], *n), active(b["q"], *n))
+
+
+def test_oracle_ct_average_order_on_alfven():
+    """On the 3-D circularly polarised Alfven wave the reference's two-point
+    CT face average converges at second order, the four-point option at
+    fourth (8^3 -> 16^3, one wave period)."""
+    import how_mhd as hm
+    lib = oracle_lib()
+
+    def err(n, pts):
+        T = float(1.0 / np.sqrt(3.0))
+        p = hm.make_parameters(nx=n, ny=n, nz=n, nt=1, tend=T, gam=5.0 / 3.0, cour=0.4, problem="alfven3d")
+        q0 = hm.problem_state(p)
+        lib.oracle_set_ct_avg(pts)
+        try:
+            o = CPUOracle(n, n, n)
+            o.set_state(q0)
+            rc, t, _ = o.run(T)
+            q = o.get_q(0)
+        finally:
+            lib.oracle_set_ct_avg(2)
+        a0, a1 = active(q0, n, n, n), active(q, n, n, n)
+        return np.mean([np.abs(a1[v] - a0[v]).mean() for v in (1, 2, 3, 4, 5, 6)])
+
+    o2 = np.log2(err(8, 2) / err(16, 2))
+    o4 = np.log2(err(8, 4) / err(16, 4))
+    assert o2 < 2.2, o2
+    assert o4 > 4.0, o4
