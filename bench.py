@@ -9,12 +9,17 @@ prot + ghost fills) over the whole domain; 1 zone-cycle = one active zone
 advanced by one step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--n 256] [--precision fp64|mixed]
+                  [--n 256] [--t-start 0.05] [--no-fast] [--no-e2e] [--no-cpu-baseline]
 
-`value` is device-timed with inputs resident in HBM; `e2e` goes through the
-C ABI with host (pinned) buffers: upload q + face B, tstep, ssprk, download,
-every step.  Under torchrun each rank advances its own replica (the path has
-no data exchange at one domain per GPU), time = max over ranks.
+The timed steps start from the blast evolved to t_start.  `value` is the plain
+FP64 method (the reference's), device-timed with the state resident in HBM;
+`mixed_learned` is the mixed-precision + learned-routing form over the same
+steps from the same state, with its density / energy L1 against the FP64
+leg, max |div B| and the fraction of interfaces sent to full WENO.  `e2e`
+goes through the C ABI with host (pinned) buffers: upload q + face B, tstep,
+ssprk, download, every step.  Under torchrun each rank advances its own
+replica (the path has no data exchange at one domain per GPU), time = max
+over ranks.
 """
 from __future__ import annotations
 
@@ -52,9 +57,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--t-start", type=float, default=0.05,
+                    help="simulated time the timed steps start from (the blast evolved there first)")
+    ap.add_argument("--no-fast", action="store_true", help="skip the mixed-precision + learned-routing leg")
+    ap.add_argument("--workload", default="blast", choices=["blast", "ensemble", "accuracy"],
+                    help="ensemble: 64 uneven 2-D/1-D runs batched vs advanced one by one; "
+                         "accuracy: whole blast run to --tend in every precision / routing form")
+    ap.add_argument("--tend", type=float, default=0.2, help="end time of --workload accuracy")
     return ap.parse_args()
 
 
@@ -65,11 +76,11 @@ def dist_info():
     return world, rank, local
 
 
-def workload_text(n, precision, tend=1.0e3):
+def workload_text(n, precision, tend=1.0e3, router="off"):
     # tend far beyond the timed steps so no step is shortened by the output clamp
     return (f"nx {n}\nny {n}\nnz {n}\nnt 1\ntend {tend!r}\ngam 1.6666666666666667\ncour 0.4\n"
             f"problem blast3d_b\nx1bc periodic\nx2bc periodic\nx3bc periodic\n"
-            f"rhomin 1e-6\npgmin 1e-6\nprecision {precision}\n")
+            f"rhomin 1e-6\npgmin 1e-6\nprecision {precision}\nrouter {router}\n")
 
 
 # ------------------------------------------------------------------ clocks
@@ -246,7 +257,23 @@ def load_traffic_profile(precision):
         return None
 
 
+def div4_max(b, n, d):
+    """max |div B| of face B with the 4th-order face difference the CT update
+    preserves (src/fluxct.cpp:848-876), over active cells."""
+    import numpy as np
+    s = slice(3, n + 3)
+
+    def D(f, axis):
+        def sh(k):
+            sl = [s, s, s]
+            sl[axis] = slice(3 + k, n + 3 + k)
+            return f[tuple(sl)]
+        return (9.0 / 8.0 * (sh(0) - sh(-1)) - 1.0 / 24.0 * (sh(1) - sh(-2))) / d
+    return float(np.abs(D(b[0], 0) + D(b[1], 1) + D(b[2], 2)).max())
+
+
 def bench_ours(args):
+    import ctypes
     import numpy as np
     import torch
     import how_mhd as hm
@@ -259,11 +286,6 @@ def bench_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     n = args.n
-    p = hm.read_parameters(workload_text(n, args.precision))
-    dom = hm.Domain(p)
-    dom.init_problem()
-    stream = torch.cuda.ExternalStream(dom.stream)
-
     fp64_peak = ctypes_peak(hm)
 
     def barrier():
@@ -272,37 +294,73 @@ def bench_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # The timed steps start from the blast at t_start (evolved by the fast path,
+    # so every leg starts from the same mid-run state with a shock in the box).
+    t0_prep = time.perf_counter()
+    q_start = b_start = None
+    t_start = 0.0
+    if args.t_start > 0:
+        pp = hm.read_parameters(workload_text(n, "mixed", tend=args.t_start, router="on"))
+        with hm.Domain(pp) as d:
+            d.init_problem()
+            t_start, _, _ = d.run(0.0, -1)
+            q_start = d.get_state(0)
+            b_start = d.get_face_b(0)
+    prep_s = time.perf_counter() - t0_prep
 
-    # warm-up
-    t_sim, s, _ = dom.run(0.0, args.warmup)
-    barrier()
-    sampler = ClockSampler(device_id_for_smi(local)) if rank == 0 else None
-    if sampler:
-        sampler.start()
-        time.sleep(0.5)
-    hm.lib().how_set_kernel_timing(dom._h, 1)
-    l0 = dom.kernel_launches
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    e0.record(stream)
-    t_sim, s, _ = dom.run(t_sim, args.steps)
-    e1.record(stream)
-    barrier()
-    ms = e0.elapsed_time(e1)
-    launches = dom.kernel_launches - l0
-    import ctypes
-    sweep_ms = ctypes.c_double()
-    sweep_n = ctypes.c_long()
-    hm.lib().how_get_kernel_timing(dom._h, ctypes.byref(sweep_ms), ctypes.byref(sweep_n))
-    hm.lib().how_set_kernel_timing(dom._h, 0)
-    clocks = sampler.stop() if sampler else None
-    ms = max_over_ranks(ms, world, "cuda")
+    def make_domain(precision, router):
+        p = hm.read_parameters(workload_text(n, precision, router=router))
+        dom = hm.Domain(p)
+        if q_start is not None:
+            dom.set_state(q_start)
+            dom.set_face_b(*b_start)
+        else:
+            dom.init_problem()
+        return p, dom
+
+    def timed_leg(dom, clocks_too):
+        """warm-up, then exactly K steps between barriers, CUDA events on the
+        library's stream; returns ms, launches, sweep ms, sweep launches, clocks."""
+        stream = torch.cuda.ExternalStream(dom.stream)
+        t_sim, _, _ = dom.run(t_start, args.warmup)
+        barrier()
+        sampler = ClockSampler(device_id_for_smi(local)) if (rank == 0 and clocks_too) else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.5)
+        hm.lib().how_set_kernel_timing(dom._h, 1)
+        l0 = dom.kernel_launches
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        dom.run(t_sim, args.steps)
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        launches = dom.kernel_launches - l0
+        sweep_ms = ctypes.c_double()
+        sweep_n = ctypes.c_long()
+        hm.lib().how_get_kernel_timing(dom._h, ctypes.byref(sweep_ms), ctypes.byref(sweep_n))
+        hm.lib().how_set_kernel_timing(dom._h, 0)
+        clocks = sampler.stop() if sampler else None
+        return max_over_ranks(ms, world, "cuda"), launches, sweep_ms.value, sweep_n.value, clocks
+
+    # ---- plain FP64 (the reference's method)
+    p, dom = make_domain("fp64", "off")
+    ms, launches, sweep_ms, sweep_n, clocks = timed_leg(dom, True)
     value = replica_value(world, n ** 3, args.steps, ms)
+    rho64 = None
+    if not args.no_fast and rank == 0:
+        q64 = dom.get_state(0)
+        rho64 = q64[0, 3:n + 3, 3:n + 3, 3:n + 3].copy()
+        e64 = q64[7, 3:n + 3, 3:n + 3, 3:n + 3].copy()
+        del q64
 
-    # e2e through the C ABI with pinned host buffers
+    # ---- e2e through the C ABI with pinned host buffers
     e2e = None
     if not args.no_e2e:
+        stream = torch.cuda.ExternalStream(dom.stream)
         shp = (8,) + tuple(p.shape)
         qh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
         bh = [torch.empty(tuple(p.shape), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
@@ -325,7 +383,38 @@ def bench_ours(args):
         nbytes = 8 * int(np.prod(shp)) + 3 * 8 * int(np.prod(p.shape))
         e2e = {"value": world * n ** 3 * args.steps / (ems * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "ms_per_step": ems / args.steps}
+               "ms_per_step": ems / args.steps, "path": "plain FP64 through the C ABI (how_set_state, "
+                                                         "how_tstep, how_ssprk, how_get_state)"}
+        del qh, bh
+    dom.close()
+
+    # ---- mixed precision + learned routing (the fast form), same start, same steps
+    fast = None
+    if not args.no_fast:
+        pf, domf = make_domain("mixed", "on")
+        domf.router_stats(reset=True)
+        fms, flaunch, fsw_ms, fsw_n, _ = timed_leg(domf, False)
+        full, cheap = domf.router_stats()
+        fvalue = replica_value(world, n ** 3, args.steps, fms)
+        if rank == 0:
+            qf = domf.get_state(0)
+            bf = domf.get_face_b(0)
+            rf = qf[0, 3:n + 3, 3:n + 3, 3:n + 3]
+            ef = qf[7, 3:n + 3, 3:n + 3, 3:n + 3]
+            w, thr = hm.default_router()
+            fast = {
+                "value": fvalue, "unit": UNIT, "ms_per_step": fms / args.steps,
+                "speedup_vs_plain_fp64": fvalue / value,
+                "full_weno_fraction": full / max(full + cheap, 1),
+                "l1_rho_vs_fp64": float(np.abs(rf - rho64).sum() / np.abs(rho64).sum()),
+                "l1_energy_vs_fp64": float(np.abs(ef - e64).sum() / np.abs(e64).sum()),
+                "max_div_b": div4_max(bf, n, pf.dx),
+                "router_threshold": thr, "gpu_launches": flaunch,
+                "sweep_avg_ms": fsw_ms / max(fsw_n, 1),
+                "note": "same start state and step count as the plain FP64 leg; L1 over active cells",
+            }
+            del qf, bf
+        domf.close()
 
     if world > 1:
         import torch.distributed as dist
@@ -334,18 +423,18 @@ def bench_ours(args):
     if rank != 0:
         return 0
 
-    avg_sweep_ms = sweep_ms.value / max(sweep_n.value, 1)
+    avg_sweep_ms = sweep_ms / max(sweep_n, 1)
     achieved = SWEEP_FLOP_PER_ZONE * n ** 3 / (avg_sweep_ms * 1e-3) / 1e12
     traffic = None
-    tp = load_traffic_profile(args.precision)
+    tp = load_traffic_profile("fp64")
     if tp and "dram_bytes_per_zone" in tp:
         traffic = tp["dram_bytes_per_zone"] * n ** 3
     roofline = {
-        "bound": "fp64", "unit": "TFLOP/s", "kernel": "k_sweep (fused directional WENO sweep)",
+        "bound": "fp64", "unit": "TFLOP/s", "kernel": "k_sweep (fused directional WENO sweep), plain FP64",
         "achieved": achieved, "peak": fp64_peak, "frac": achieved / fp64_peak if fp64_peak else None,
         "peak_source": "measured live: FP64 FMA-pipe probe (how_measure_fp64_peak), of measured",
         "flop_per_launch": SWEEP_FLOP_PER_ZONE * n ** 3, "avg_launch_ms": avg_sweep_ms,
-        "launches_timed": sweep_n.value, "share_of_step": sweep_ms.value / ms if ms else None,
+        "launches_timed": sweep_n, "share_of_step": sweep_ms / ms if ms else None,
         "traffic": traffic,
         "step_frac": value / world * FLOP_PER_ZONE_CYCLE / (fp64_peak * 1e12) if fp64_peak else None,
     }
@@ -357,19 +446,150 @@ def bench_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"3-D MHD blast {n}^3 (blast3d_b), periodic, gam 5/3, cour 0.4, floors 1e-6; "
-                               f"SSPRK(5,4) + characteristic WENO5/LLF + 4th-order CT",
-                   "n": n, "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
+                               f"SSPRK(5,4) + characteristic WENO5/LLF + 4th-order CT; `value` = plain FP64, "
+                               f"`mixed_learned` = FP32 characteristic part + learned WENO routing",
+                   "n": n, "t_start": t_start, "prep_s": prep_s,
+                   "parallelism": "replicas" if world > 1 else "single",
                    "l2": "state 12.5 GB per replica >> 126 MB L2: every step streams from HBM, no flush"},
         "roofline": roofline,
+        "mixed_learned": fast,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- ensemble arm
+def ensemble_members(hm, seed=2024):
+    """The batched-ensemble workload: 24 Orszag-Tang vortices and 24 MHD rotors
+    at sizes drawn from {64^2, 128^2, 256^2, 512^2} (gamma ~ U[1.4, 1.7] for
+    the vortices), 16 Brio-Wu tubes of nx in {400, 800, 1600} (gamma 2, open)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sizes = [64, 128, 256, 512]
+    P = hm.make_parameters
+    out = []
+    for _ in range(24):
+        n = int(rng.choice(sizes))
+        out.append(P(nx=n, ny=n, nz=1, nt=1, tend=0.5, gam=float(rng.uniform(1.4, 1.7)), cour=0.4,
+                     problem="orszag_tang"))
+    for _ in range(24):
+        n = int(rng.choice(sizes))
+        out.append(P(nx=n, ny=n, nz=1, nt=1, tend=0.15, gam=1.4, cour=0.4, problem="mhd_rotor",
+                     x1bc="open", x2bc="open", x3bc="periodic"))
+    for _ in range(16):
+        n = int(rng.choice([400, 800, 1600]))
+        out.append(P(nx=n, ny=1, nz=1, nt=1, tend=0.1, gam=2.0, cour=0.4, problem="brio_wu",
+                     x1bc="open", x2bc="open", x3bc="open"))
+    return out
+
+
+def bench_ensemble(args):
+    """Aggregate zone-cycles/s of the 64-member ensemble over K steps of every
+    member: batched (one launch per kernel for all members, one CUDA graph per
+    step, autotuned tile shapes) against the same members advanced one by one
+    through how_run.  Replicas only under torchrun."""
+    import torch
+    import how_mhd as hm
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    members = ensemble_members(hm)
+    zones = sum(p.nx * p.ny * p.nz for p in members)
+    with hm.Ensemble(members) as e:
+        e.init()
+        e.run(args.warmup + 3)               # autotune (3 steps) + warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.run(args.steps)
+        torch.cuda.synchronize()
+        ens_s = time.perf_counter() - t0
+        shapes, sweep_ms = e.shapes()
+        launches = e.graph_launches
+    # one by one, same K steps per member (each with its own warm-up)
+    seq_s = 0.0
+    for p in members:
+        with hm.Domain(p) as d:
+            d.init_problem()
+            t, _, _ = d.run(0.0, args.warmup)
+            d.sync()
+            t0 = time.perf_counter()
+            d.run(t, args.steps)
+            d.sync()
+            seq_s += time.perf_counter() - t0
+    if rank != 0:
+        return 0
+    value = world * zones * args.steps / ens_s
+    line = {
+        "metric": "zone-cycles/s, batched ensemble of 64 uneven 2-D/1-D runs, 1 B200", "value": value,
+        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * ens_s / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "24 Orszag-Tang + 24 MHD rotors at {64..512}^2, 16 Brio-Wu at nx {400,800,1600}",
+                   "members": len(members), "zones": zones, "timing": "host clock around synchronised runs"},
+        "one_by_one": {"value": world * zones * args.steps / seq_s, "unit": UNIT, "seconds": seq_s},
+        "speedup_vs_one_by_one": seq_s / ens_s,
+        "tile_shapes": {d: hm.Ensemble.shape_info(d, s) for d, s in zip("xyz", shapes)},
+        "autotune_sweep_ms": sweep_ms.tolist(),
+        "graph_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- accuracy arm
+def bench_accuracy(args):
+    """The blast from t = 0 to --tend in plain FP64, mixed precision, mixed +
+    learned routing and mixed + guard-only routing: density / energy L1 of each
+    against FP64, max |div B|, ms per step and the fraction of interfaces sent
+    to full WENO."""
+    import numpy as np
+    import torch
+    import how_mhd as hm
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    n = args.n
+    s = slice(3, n + 3)
+    w, thr = hm.default_router()
+    forms = [("fp64", "fp64", None), ("mixed", "mixed", None), ("mixed+learned", "mixed", "learned"),
+             ("mixed+guard", "mixed", "guard")]
+    out, ref = {}, None
+    for name, prec, mode in forms:
+        p = hm.read_parameters(workload_text(n, prec, tend=args.tend))
+        with hm.Domain(p) as d:
+            d.init_problem()
+            if mode:
+                d.set_router(w, mode, threshold=thr)
+            d.sync()
+            t0 = time.perf_counter()
+            t, steps, _ = d.run(0.0, -1)
+            d.sync()
+            el = time.perf_counter() - t0
+            q = d.get_state(0)
+            b = d.get_face_b(0)
+            st = d.router_stats() if mode else None
+        rho, en = q[0, s, s, s].copy(), q[7, s, s, s].copy()
+        del q
+        r = {"steps": steps, "t": t, "ms_per_step": 1e3 * el / steps, "zone_cycles_per_s": n ** 3 * steps / el,
+             "max_div_b": div4_max(b, n, p.dx), "max_abs_b": float(max(np.abs(x).max() for x in b))}
+        if st:
+            r["full_weno_fraction"] = st[0] / max(st[0] + st[1], 1)
+        if ref is None:
+            ref = (rho, en)
+        else:
+            r["l1_rho_vs_fp64"] = float(np.abs(rho - ref[0]).sum() / np.abs(ref[0]).sum())
+            r["l1_energy_vs_fp64"] = float(np.abs(en - ref[1]).sum() / np.abs(ref[1]).sum())
+        out[name] = r
+        del b
+    if rank == 0:
+        print(json.dumps({"workload": f"blast3d_b {n}^3, t = 0 .. {args.tend}", "router_threshold": thr,
+                          "timing": "host clock around the synchronised run (tstep + ssprk every step)",
+                          "forms": out}), flush=True)
     return 0
 
 
@@ -384,6 +604,10 @@ def main():
     args = parse()
     if args.impl == "reference":
         return bench_reference(args)
+    if args.workload == "ensemble":
+        return bench_ensemble(args)
+    if args.workload == "accuracy":
+        return bench_accuracy(args)
     return bench_ours(args)
 
 

@@ -149,6 +149,8 @@ void launch_init_faceb(Ctx& c);
 void launch_tstep(Ctx& c, double time, double target, int clamp);
 void launch_set_dt(Ctx& c);     // dt already in dsc->dt: fill dtdl
 void launch_sweep(Ctx& c, int dir, const SweepArgs& a);
+// learned-router decisions of every interface of sweep `dir` (route_prepass.cu)
+void launch_route(Ctx& c, int dir, const double* q, const unsigned char* prev, unsigned char* next);
 void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5);
 void launch_faceb_base(Ctx& c, int iw, double c4, double c5, int stage5);
 void launch_prot(Ctx& c, int stage);

@@ -102,17 +102,17 @@ int how_sweep_phase_profile(how_ctx* cp, int dir, double dt, double* out, int no
     Ctx* c = cp;
     if (!c || !out) return HOW_ERR_ARG;
     unsigned long long* d = nullptr;
-    HOW_CUDA_CHECK(cudaMalloc(&d, 8 * sizeof(unsigned long long)));
-    HOW_CUDA_CHECK(cudaMemset(d, 0, 8 * sizeof(unsigned long long)));
+    HOW_CUDA_CHECK(cudaMalloc(&d, 12 * sizeof(unsigned long long)));
+    HOW_CUDA_CHECK(cudaMemset(d, 0, 12 * sizeof(unsigned long long)));
     c->prof = d;
     const int rc = how_sweep(cp, dir, dt);
     c->prof = nullptr;
-    unsigned long long h[8] = {0};
+    unsigned long long h[12] = {0};
     cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (rc) return rc;
-    for (int k = 0; k < nout && k < 8; ++k)
-        out[k] = k < 7 ? (h[7] ? (double)h[k] / (double)h[7] : 0.0) : (double)h[7];
+    for (int k = 0; k < nout && k < 12; ++k)
+        out[k] = k < 11 ? (h[11] ? (double)h[k] / (double)h[11] : 0.0) : (double)h[11];
     return HOW_OK;
 }
 

@@ -1,0 +1,215 @@
+// route_prepass.cu -- the learned router's decisions for every interface of a
+// sweep, computed before the sweep in one batched pass.
+//
+// The routing values of each interface's 6 stencil cells come from the stage
+// input (the sweep's primitive floors; fast speed along the sweep normal),
+// then the 6 features and the guard (router.cuh); a warp's 32 interfaces are
+// two 16-row groups of the BF16 tensor-core network.  Groups whose stencils
+// are all uniform take the precomputed logit of a flat stencil.
+// The decision (1: full characteristic WENO) lands in the per-face byte array
+// the sweep reads and the next stage's prior comes from.
+#include "how_internal.cuh"
+#include "router.cuh"
+
+namespace how {
+
+namespace {
+
+__device__ __forceinline__ int route_perm(int dir, int v) {
+    // line variable v -> conserved index (x: identity; y: rho,My,Mz,Mx,By,Bz,Bx,E;
+    // z: rho,Mz,Mx,My,Bz,Bx,By,E), the sweeps' order
+    return dir == 0 ? v
+         : dir == 1 ? (v == 1 ? 2 : v == 2 ? 3 : v == 3 ? 1 : v == 4 ? 5 : v == 5 ? 6 : v == 6 ? 4 : v)
+                    : (v == 1 ? 3 : v == 2 ? 1 : v == 3 ? 2 : v == 4 ? 6 : v == 5 ? 4 : v == 6 ? 5 : v);
+}
+
+struct RouteArgs {
+    Grid g;
+    const double* q;            // stage input, field 0 (var v at + v * fs)
+    const unsigned char* prev;  // previous decisions of this direction (the prior)
+    unsigned char* next;        // this sweep's decisions
+    const float* w;             // network (RouterLayout)
+    float thr, guard_jump, guard_floor;
+    double gam, rhomin, pgmin;
+    unsigned long long* groups; // [0] tensor-core groups, [1] flat groups (may be null)
+};
+
+constexpr int kRouteThreads = 256;
+
+// Routing values of one cell: floored density and pressure (the sweep's
+// primit floors, src/ssprk.cpp:479-512), |B|, |v| and the fast speed along
+// the sweep normal, in the sweep's arithmetic order.
+__device__ __forceinline__ StencilCell route_cell(const double* q, long long fs, long long c, int dir, double gam,
+                                                  double rhomin, double pgmin) {
+    const double DD = q[c];
+    const double Mx = q[route_perm(dir, 1) * fs + c], My = q[route_perm(dir, 2) * fs + c];
+    const double Mz = q[route_perm(dir, 3) * fs + c];
+    const double Bx = q[route_perm(dir, 4) * fs + c], By = q[route_perm(dir, 5) * fs + c];
+    const double Bz = q[route_perm(dir, 6) * fs + c];
+    const double EE = q[7 * fs + c];
+    double rho = DD;
+    double irho = 1.0 / rho;
+    const double vx = Mx * irho, vy = My * irho, vz = Mz * irho;
+    const double vv2 = vx * vx + vy * vy + vz * vz;
+    const double BB2 = Bx * Bx + By * By + Bz * Bz;
+    double pg = (gam - 1.0) * (EE - 0.5 * (rho * vv2 + BB2));
+    if (rho < rhomin || pg < pgmin) {
+        rho = fmax(rhomin, rho);
+        pg = fmax(pgmin, pg);
+        irho = 1.0 / rho;
+    }
+    const double bbn2 = BB2 * irho;
+    const double bnx2 = Bx * Bx * irho;
+    const double cs2 = fmax(0.0, gam * fabs(pg * irho));
+    const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
+    const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
+    return StencilCell{(float)rho, (float)pg, sqrtf((float)BB2), sqrtf((float)vv2), (float)lf};
+}
+
+// Each thread walks one segment of kSeg interfaces of one line along the
+// sweep direction with a sliding window of its 6 stencil cells, so every cell's
+// routing values are formed once per segment (kSeg + 5 cells for kSeg faces).
+// Lanes of a warp hold consecutive lines (x-adjacent for the y and z sweeps:
+// coalesced loads), and at every step the warp's 32 interfaces are two 16-row
+// groups of the network.
+constexpr int kSeg = 32;
+
+template <int DIR>
+__global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__ RouteArgs a) {
+    __shared__ RouterSmem rs;
+    __shared__ __align__(16) __nv_bfloat16 X[kRouteThreads / 32][32][16];
+    __shared__ float lg[kRouteThreads / 32][32];
+    __shared__ float flat_logit[2];
+    __shared__ unsigned int cnt[2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    router_load_smem(&rs, a.w, tid, blockDim.x);
+    if (tid < 2) cnt[tid] = 0u;
+    __syncthreads();
+    if (warp == 0) {
+        // logits of a uniform stencil with prior 0 and 1, through the same code
+        StencilCell sc[6];
+        const float u = (float)a.gam;
+        for (int k = 0; k < 6; ++k) sc[k] = StencilCell{u, u, u, u, u};
+        float ff[kRouterNF];
+        bool flat;
+        router_features(sc, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, ff, &flat);
+        for (int e = lane; e < 256; e += 32) {
+            const int r = e / 16, k = e % 16;
+            X[0][r][k] = __float2bfloat16_rn(k < 5 ? ff[k] : k == 5 ? (float)(r & 1) : 0.0f);
+        }
+        __syncwarp();
+        router_mma_16rows(&rs, X[0], lg[0]);
+        __syncwarp();
+        if (lane < 2) flat_logit[lane] = lg[0][lane];
+    }
+    __syncthreads();
+
+    const Grid& g = a.g;
+    const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
+    const long long stride = DIR == 0 ? 1ll : DIR == 1 ? (long long)g.pitch : (long long)g.pitch * g.P1;
+    // lines: DIR 0 (j, k); DIR 1 (i, k); DIR 2 (i, j) -- the faster index first
+    const int la = DIR == 0 ? g.ny : g.nx;
+    const int lb = DIR == 2 ? g.ny : g.nz;
+    const long long nlines = (long long)la * lb;
+    const int nseg = (n + 1 + kSeg - 1) / kSeg;
+    const long long nwork = nlines * nseg;   // (segment, line), line fastest
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < nwork; base += (long long)gridDim.x * blockDim.x) {
+        const long long widx = base + tid;
+        const bool valid = widx < nwork;
+        long long line = 0;
+        int f0 = 0;
+        if (valid) {
+            const long long ln = widx % nlines;
+            f0 = (int)(widx / nlines) * kSeg;
+            const int ia = (int)(ln % la), ib = (int)(ln / la);
+            line = DIR == 0 ? g.idx(0, 3 + ia, 3 + ib) : DIR == 1 ? g.idx(3 + ia, 0, 3 + ib) : g.idx(3 + ia, 3 + ib, 0);
+        }
+        // window: stencil cells f .. f+5 of face f (padded cells)
+        StencilCell win[6];
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+                win[k] = route_cell(a.q, g.fs, line + (long long)(f0 + k) * stride, DIR, a.gam, a.rhomin, a.pgmin);
+        }
+        for (int s = 0; s < kSeg; ++s) {
+            const int iface = f0 + s;
+            const bool live = valid && iface <= n;
+            float ft[kRouterNF] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            bool flat = true, guard = false;
+            const long long face = line + (long long)(iface + 2) * stride;
+            if (live) {
+                win[5] = route_cell(a.q, g.fs, line + (long long)(iface + 5) * stride, DIR, a.gam, a.rhomin, a.pgmin);
+                const float prior = (float)a.prev[face];
+                guard = router_features(win, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump, a.guard_floor, ft,
+                                        &flat);
+#pragma unroll
+                for (int k = 0; k < 5; ++k) win[k] = win[k + 1];
+            }
+            uint4 v0;
+            v0.x = pack_bf16(ft[0], ft[1]); v0.y = pack_bf16(ft[2], ft[3]);
+            v0.z = pack_bf16(ft[4], ft[5]); v0.w = 0u;
+            reinterpret_cast<uint4*>(&X[warp][lane][0])[0] = v0;
+            reinterpret_cast<uint4*>(&X[warp][lane][0])[1] = make_uint4(0u, 0u, 0u, 0u);
+            const int code = flat ? 1 + (ft[5] > 0.5f ? 1 : 0) : 0;
+            // every lane of the warp reaches here kSeg times (uniform trip count)
+            __syncwarp();
+            float logit = 0.0f;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const unsigned int nonflat = __ballot_sync(0xffffffffu, code == 0);
+                const unsigned int half = h == 0 ? 0x0000ffffu : 0xffff0000u;
+                if ((nonflat & half) == 0u) {
+                    if ((lane >> 4) == h) logit = flat_logit[code - 1];
+                    if (lane == 0) atomicAdd(&cnt[1], 1u);
+                } else {
+                    router_mma_16rows(&rs, X[warp] + 16 * h, lg[warp] + 16 * h);
+                    __syncwarp();
+                    if ((lane >> 4) == h) logit = lg[warp][lane];
+                    if (lane == 0) atomicAdd(&cnt[0], 1u);
+                }
+            }
+            if (live) a.next[face] = (guard || logit > a.thr) ? 1 : 0;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && a.groups) {
+        atomicAdd(&a.groups[0], (unsigned long long)cnt[0]);
+        atomicAdd(&a.groups[1], (unsigned long long)cnt[1]);
+    }
+}
+
+}  // namespace
+
+// Decisions of sweep `dir` over stage input q into c.route_prev's write half.
+void launch_route(Ctx& c, int dir, const double* q, const unsigned char* prev, unsigned char* next) {
+    RouteArgs a;
+    a.g = c.g;
+    a.q = q;
+    a.prev = prev;
+    a.next = next;
+    a.w = c.router_w;
+    a.thr = c.route_thr;
+    a.guard_jump = c.guard_jump;
+    a.guard_floor = c.guard_floor;
+    a.gam = c.p.gam;
+    a.rhomin = c.p.rhomin;
+    a.pgmin = c.p.pgmin;
+    a.groups = c.route_count ? c.route_count + 2 : nullptr;
+    const Grid& g = c.g;
+    const int n = dir == 0 ? g.nx : dir == 1 ? g.ny : g.nz;
+    const long long nlines = dir == 0 ? (long long)g.ny * g.nz : dir == 1 ? (long long)g.nx * g.nz
+                                                                        : (long long)g.nx * g.ny;
+    const long long nwork = nlines * ((n + 1 + kSeg - 1) / kSeg);
+    long long blocks = (nwork + kRouteThreads - 1) / kRouteThreads;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
+    if (blocks > (long long)nsm * 8) blocks = (long long)nsm * 8;
+    if (blocks < 1) blocks = 1;
+    if (dir == 0) k_route<0><<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
+    else if (dir == 1) k_route<1><<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
+    else k_route<2><<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
+    ++c.launches;
+}
+
+}  // namespace how

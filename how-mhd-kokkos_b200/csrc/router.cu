@@ -288,8 +288,8 @@ int how_router_configure(how_ctx* c, int mode, float threshold, float guard_jump
         HOW_CUDA_CHECK(cudaMemset(c->route_prev, 1, 6 * (size_t)c->g.fs));
     }
     if (!c->route_count) {
-        HOW_CUDA_CHECK(cudaMalloc(&c->route_count, 2 * sizeof(unsigned long long)));
-        HOW_CUDA_CHECK(cudaMemset(c->route_count, 0, 2 * sizeof(unsigned long long)));
+        HOW_CUDA_CHECK(cudaMalloc(&c->route_count, 4 * sizeof(unsigned long long)));
+        HOW_CUDA_CHECK(cudaMemset(c->route_count, 0, 4 * sizeof(unsigned long long)));
     }
     c->route_mode = mode;
     c->route_thr = threshold;
@@ -300,9 +300,18 @@ int how_router_configure(how_ctx* c, int mode, float threshold, float guard_jump
 
 // Interfaces (active faces) sent to full WENO and to the linear flux since
 // the last reset.
+int how_router_stats4(how_ctx* c, unsigned long long* full, unsigned long long* cheap,
+                      unsigned long long* mma_groups, unsigned long long* flat_groups, int reset);
 int how_router_stats(how_ctx* c, unsigned long long* full, unsigned long long* cheap, int reset) {
+    return how_router_stats4(c, full, cheap, nullptr, nullptr, reset);
+}
+
+// ... and the 16-interface groups whose logits came from the tensor cores or,
+// all their stencils being uniform, from the precomputed flat logits.
+int how_router_stats4(how_ctx* c, unsigned long long* full, unsigned long long* cheap,
+                      unsigned long long* mma_groups, unsigned long long* flat_groups, int reset) {
     if (!c) return HOW_ERR_ARG;
-    unsigned long long h[2] = {0, 0};
+    unsigned long long h[4] = {0, 0, 0, 0};
     if (c->route_count) {
         HOW_CUDA_CHECK(cudaStreamSynchronize(c->stream));
         HOW_CUDA_CHECK(cudaMemcpy(h, c->route_count, sizeof(h), cudaMemcpyDeviceToHost));
@@ -310,6 +319,8 @@ int how_router_stats(how_ctx* c, unsigned long long* full, unsigned long long* c
     }
     if (full) *full = h[0];
     if (cheap) *cheap = h[1];
+    if (mma_groups) *mma_groups = h[2];
+    if (flat_groups) *flat_groups = h[3];
     return HOW_OK;
 }
 

@@ -57,8 +57,10 @@ __device__ __forceinline__ float gelu_fast(float x) {
 // Features from the stencil's cell values; returns the guard decision.
 struct StencilCell { float rho, p, bmag, vmag, cf; };
 
+// *flat: every jump is exactly zero (a uniform stencil), so feat[0..4] are all
+// log10f(1e-6f).
 __device__ __forceinline__ bool router_features(const StencilCell* s, float prior, float rhomin, float pgmin,
-                                                float guard_jump, float guard_floor, float* feat) {
+                                                float guard_jump, float guard_floor, float* feat, bool* flat) {
     float minrho = s[0].rho, minp = s[0].p, maxb = s[0].bmag, maxcf = s[0].cf, mincf = s[0].cf;
     float drho = 0.f, dp = 0.f, db = 0.f, dv = 0.f, dcf = 0.f;
 #pragma unroll
@@ -79,6 +81,7 @@ __device__ __forceinline__ bool router_features(const StencilCell* s, float prio
     feat[3] = log10f(1e-6f + dv / fmaxf(maxcf, tiny));
     feat[4] = log10f(1e-6f + dcf / fmaxf(mincf, tiny));
     feat[5] = prior;
+    *flat = drho == 0.0f && dp == 0.0f && db == 0.0f && dv == 0.0f && dcf == 0.0f;
     const bool bad = !(jr == jr) || !(jp == jp);   // NaN anywhere: full method
     return bad || jr > guard_jump || jp > guard_jump || minrho < guard_floor * rhomin ||
            minp < guard_floor * pgmin;

@@ -102,20 +102,18 @@ struct Tile {
     static constexpr int szS0 = (int)sizeof(R) * NS * NI;
     static constexpr int szS1 = offdF + 8 * 7 * NI;
     static constexpr int bB = bS + align_up(szS0 > szS1 ? szS0 : szS1, 16);   // 3 mbarriers
-    // routing (MODE 1-3): decision, compacted list, weight deviation, FP32
-    // features of the tile's interfaces, the network; BF16 features and logits
-    // of the routing phase live in the L/R region (free between P1b and P2b)
-    static constexpr int NRp = align_up(NLF, 16);                 // MMA row padding
+    // routing (MODE 1-3): decision, compacted list, weight deviation and FP32
+    // features of the tile's interfaces (collection), the linear flux's LF
+    // speed, the cells' routing values (guard and collection)
     static constexpr int bDec = bB + 32;                          // [NLF] int
-    static constexpr int bList = bDec + align_up(4 * NLF, 16);    // [NRp] int
-    static constexpr int bDev = bList + align_up(4 * NRp, 16);    // [NLF] float (bits)
+    static constexpr int bList = bDec + align_up(4 * NLF, 16);    // [NLF] int
+    static constexpr int bDev = bList + align_up(4 * NLF, 16);    // [NLF] float (bits)
     static constexpr int bFt = bDev + align_up(4 * NLF, 16);      // [NLF][6] float
-    static constexpr int bRS = bFt + align_up(4 * 6 * NLF, 16);   // RouterSmem
-    static constexpr int bX = bL;                                 // [NRp][16] bf16 (aliases L/R)
-    static constexpr int bLogit = bL + align_up(2 * 16 * NRp, 16); // [NRp] float (aliases L/R)
+    static constexpr int bAmx = bFt + align_up(4 * 6 * NLF, 16);  // [NLF] R: linear-flux LF speed
+    static constexpr int bCF = bAmx + align_up((int)sizeof(R) * NLF, 16);   // [5][NLC] float cell features
+    static constexpr int bEnd = bCF + align_up(4 * 5 * NLC, 16);
     static constexpr size_t bytes_plain = (size_t)bB + 3 * 8;
-    static constexpr size_t bytes_route = (size_t)bRS + sizeof(RouterSmem);
-    static_assert(2 * 16 * NRp + 4 * NRp <= szLR, "routing scratch must fit the L/R region");
+    static constexpr size_t bytes_route = (size_t)bEnd;
     static constexpr uint32_t in_bytes = 8u * NQ;
     static constexpr uint32_t out_bytes = 8u * NO;
 };
@@ -198,8 +196,8 @@ __device__ __forceinline__ R weno_flux_d(const R* dF, const R* dq, R amx, R* dev
 }
 
 // Component-wise fifth-order upwind flux with the linear weights
-// (0.1, 0.6, 0.3) and a global Lax-Friedrichs speed: the cheap flux a
-// router sends smooth interfaces to.  dF_k, dq_k are the physical cell
+// (0.1, 0.6, 0.3) and the stencil's largest |lambda| as Lax-Friedrichs speed:
+// the cheap flux a router sends smooth interfaces to.  dF_k, dq_k are the physical cell
 // differences of one component over the stencil; returns the correction to
 // the central F_i (same form as weno_flux_d, no characteristic projection).
 template <typename R>
@@ -255,11 +253,10 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     int* sList = reinterpret_cast<int*>(sm + TL::bList);        // full-WENO interfaces, compacted
     float* sDev = reinterpret_cast<float*>(sm + TL::bDev);      // weight deviation (collect)
     float* sFt = reinterpret_cast<float*>(sm + TL::bFt);        // features (collect)
-    RouterSmem* sRS = reinterpret_cast<RouterSmem*>(sm + TL::bRS);
-    __nv_bfloat16 (*sX)[16] = reinterpret_cast<__nv_bfloat16 (*)[16]>(sm + TL::bX);
-    float* sLogit = reinterpret_cast<float*>(sm + TL::bLogit);
+    R* sAmx = reinterpret_cast<R*>(sm + TL::bAmx);              // per interface: max |lambda_0|, |lambda_6|
+    float* sCF = reinterpret_cast<float*>(sm + TL::bCF);        // per cell: rho, p, |B|, |v|, c_f (routing)
     __shared__ int s_nfull;
-    __shared__ unsigned int s_cnt[2];
+    __shared__ unsigned int s_cnt[2];   // full, cheap interfaces
 
     // Tiles: T active cells along the sweep x NL lines x one plane.  Lines of
     // the x sweep start at j = 3; lines of the y/z sweeps are consecutive i and
@@ -325,29 +322,6 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         mbar_init(&bars[2], 1);
         fence_barrier_init();
     }
-    // MODE 1: the network in shared memory, and its logits for a flat stencil
-    // (every jump feature at its floor) with prior 0 and 1: rows of a tile
-    // whose 16 interfaces are all flat take these instead of a tensor-core
-    // pass (the MMA rows are independent, so the values are the same)
-    __shared__ float s_flat_logit[2];
-    float flat_feature = 0.0f;
-    if constexpr (MODE == 1) {
-        flat_feature = log10f(1e-6f + 0.0f);
-        router_load_smem(sRS, a0.router, tid, blockDim.x);
-        __syncthreads();
-        if (tid < 32) {
-            __nv_bfloat16 (*X)[16] = reinterpret_cast<__nv_bfloat16 (*)[16]>(sm + TL::bX);
-            float* lg = reinterpret_cast<float*>(sm + TL::bLogit);
-            for (int e = tid; e < 256; e += 32) {
-                const int r = e / 16, k = e % 16;
-                X[r][k] = __float2bfloat16_rn(k < 5 ? flat_feature : k == 5 ? (float)(r & 1) : 0.0f);
-            }
-            __syncwarp();
-            router_mma_16rows(sRS, X, lg);
-            __syncwarp();
-            if (tid < 2) s_flat_logit[tid] = lg[tid];
-        }
-    }
     __syncthreads();
 
     // TMA loads (thread 0 only): the raw tile of `tile` into buffer b
@@ -411,7 +385,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         if (a0.prof != nullptr && tid == 0) {
             const long long now = clock64();
             atomicAdd(a0.prof + ph, (unsigned long long)(now - tprev));
-            if (ph == 6) atomicAdd(a0.prof + 7, 1ull);   // tiles
+            if (ph == 10) atomicAdd(a0.prof + 11, 1ull);   // tiles
             tprev = now;
         }
     };
@@ -465,6 +439,16 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 pend_bits |= 1u << (buf ^ 1);
             }
         }
+        // MODE 1: this tile's routing decisions (formed by the routing pass),
+        // loaded now so their latency hides behind P1
+        int pre_dec = 0;
+        if constexpr (MODE == 1) {
+            if (tid < NLF) {
+                const int l = tid / F, f = tid % F;
+                const int iface = c0 + f;
+                if (line_ok(l) && iface <= n) pre_dec = a.route_next[line_off(l) + (long long)(iface + 2) * sstride];
+            }
+        }
         mark(0);
 
         // ------------------------------------------------------------ P1
@@ -499,6 +483,14 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             const double cs2 = fmax(0.0, gam * fabs(pg * irho));
             const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
             const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
+            if constexpr (MODE == 2 || MODE == 3) {
+                // the routing features' cell values, once per cell
+                sCF[0 * NLC + t] = (float)rho;
+                sCF[1 * NLC + t] = (float)pg;
+                sCF[2 * NLC + t] = sqrtf((float)BB2);
+                sCF[3 * NLC + t] = sqrtf((float)vv2);
+                sCF[4 * NLC + t] = (float)lf;
+            }
             const double la = sqrt(fmax(0.0, bnx2));
             const double ls = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 - root)));
             sA[0 * NLC + t] = R(vx - lf); sA[1 * NLC + t] = R(vx - la); sA[2 * NLC + t] = R(vx - ls);
@@ -525,73 +517,68 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             const int c = (t / 14) % C;
             sD[t] = (c + 1 < C) ? R(sUst[t + 14] - sUst[t]) : R(0);
         }
+        if constexpr (MODE != 0) {
+            if (tid < 2) s_cnt[tid] = 0u;
+        }
         __syncthreads();
+        mark(2);
 
         // ------------------------------------------------------------ PR
         // routing: features of every interface, the hard guard, the network
         // (MODE 1), and the compacted list of interfaces that get full WENO
         int nfull = NLF;
         if constexpr (MODE != 0) {
-            if (tid < 2) s_cnt[tid] = 0u;
-            for (int t = tid; t < TL::NRp; t += blockDim.x) {
-                if (t >= NLF) {
-                    if constexpr (MODE == 1) {
-#pragma unroll
-                        for (int k = 0; k < 16; ++k) sX[t][k] = __float2bfloat16_rn(0.0f);
-                        sList[t] = 1;   // padding row: its logit is never read
-                    }
-                    continue;
-                }
+            // features of interface t (tile-local), its guard and its flatness
+            auto row_features = [&](int t, float* ft, bool& flat, float& prior) -> bool {
                 const int l = t / F, f = t % F;
                 StencilCell sc[6];
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
-                    const int c = l * C + f + k;
-                    const double vx = sP[1 * NLC + c], vy = sP[2 * NLC + c], vz = sP[3 * NLC + c];
-                    const double Bx = sP[4 * NLC + c], By = sP[5 * NLC + c], Bz = sP[6 * NLC + c];
-                    sc[k].rho = (float)sP[0 * NLC + c];
-                    sc[k].p = (float)sP[7 * NLC + c];
-                    sc[k].bmag = (float)sqrt(Bx * Bx + By * By + Bz * Bz);
-                    sc[k].vmag = (float)sqrt(vx * vx + vy * vy + vz * vz);
-                    sc[k].cf = (float)(sA[6 * NLC + c] - sA[3 * NLC + c]);
+                    const int cc = l * C + f + k;
+                    sc[k] = StencilCell{sCF[0 * NLC + cc], sCF[1 * NLC + cc], sCF[2 * NLC + cc], sCF[3 * NLC + cc],
+                                        sCF[4 * NLC + cc]};
                 }
                 const int iface = c0 + f;
-                float prior = 1.0f;
+                prior = 1.0f;
                 if (line_ok(l) && iface <= n) prior = (float)a.route_prev[line_off(l) + (long long)(iface + 2) * sstride];
-                float ft[kRouterNF];
-                const bool guard = router_features(sc, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump,
-                                                   a.guard_floor, ft);
-                if constexpr (MODE == 1) {
+                return router_features(sc, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump, a.guard_floor, ft,
+                                       &flat);
+            };
+            // Lax-Friedrichs speed of the linear flux: the stencil's largest |lambda|
+            auto row_amx = [&](int t) {
+                const int cb = (t / F) * C + t % F;
+                R amx = fmax(fabs(sA[0 * NLC + cb]), fabs(sA[6 * NLC + cb]));
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) sX[t][k] = __float2bfloat16_rn(k < kRouterNF ? ft[k] : 0.0f);
-                    // flat code (scratch in sList until compaction): 0 not flat, 1 + prior
-                    const bool flat = ft[0] == flat_feature && ft[1] == flat_feature && ft[2] == flat_feature &&
-                                      ft[3] == flat_feature && ft[4] == flat_feature;
-                    sList[t] = flat ? 1 + (prior > 0.5f ? 1 : 0) : 0;
-                }
-                if constexpr (MODE == 3) {
-#pragma unroll
-                    for (int k = 0; k < kRouterNF; ++k) sFt[t * 6 + k] = ft[k];
-                    sDev[t] = 0.0f;
-                }
-                sDec[t] = MODE == 3 ? 1 : (guard ? 1 : 0);
-            }
-            __syncthreads();
+                for (int k = 1; k < 6; ++k) amx = fmax(amx, fmax(fabs(sA[0 * NLC + cb + k]), fabs(sA[6 * NLC + cb + k])));
+                sAmx[t] = amx;
+            };
             if constexpr (MODE == 1) {
-                const int w = tid >> 5, nw = blockDim.x >> 5;
-                const int lane = tid & 31;
-                for (int mt = w; mt < TL::NRp / 16; mt += nw) {
-                    const int code = lane < 16 ? sList[16 * mt + lane] : 1;
-                    if (__all_sync(0xffffffffu, code != 0)) {
-                        if (lane < 16) sLogit[16 * mt + lane] = s_flat_logit[code - 1];
-                    } else {
-                        router_mma_16rows(sRS, sX + 16 * mt, sLogit + 16 * mt);
-                    }
+                // decisions of the learned router, formed for the whole sweep by
+                // the routing pass (route_prepass.cu) before this launch
+                static_assert(NLF <= NT, "one decision per thread");
+                if (tid < NLF) {
+                    sDec[tid] = pre_dec;
+                    row_amx(tid);
                 }
                 __syncthreads();
-                for (int t = tid; t < NLF; t += blockDim.x)
-                    if (sLogit[t] > a.route_thr) sDec[t] = 1;
+                mark(3);
+                mark(4);
+            } else {
+                for (int t = tid; t < NLF; t += blockDim.x) {
+                    float ft[kRouterNF];
+                    bool flat;
+                    float prior;
+                    const bool guard = row_features(t, ft, flat, prior);
+                    if constexpr (MODE == 2) row_amx(t);
+                    if constexpr (MODE == 3) {
+#pragma unroll
+                        for (int k = 0; k < kRouterNF; ++k) sFt[t * 6 + k] = ft[k];
+                        sDev[t] = 0.0f;
+                    }
+                    sDec[t] = MODE == 3 ? 1 : (guard ? 1 : 0);
+                }
                 __syncthreads();
+                mark(3);
             }
             if constexpr (ROUTED) {
                 if (tid < 32) {   // compaction by one warp
@@ -609,6 +596,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 nfull = s_nfull;
             }
         }
+
+        mark(5);
 
         // ------------------------------------------------------------ P2a
         for (int k = tid; k < nfull; k += blockDim.x) {
@@ -659,7 +648,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             S[S_ICS2 * NI] = Math<R>::rcp(cs2);
         }
         __syncthreads();
-        mark(2);
+        mark(6);
 
         // ------------------------------------------------------------ P2b
         for (int t = tid; t < 7 * nfull; t += blockDim.x) {
@@ -775,7 +764,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             for (int m = 0; m < 7; ++m) { lo[m * NI] = L[m] * sg; ro[m * NI] = Rv[m] * sg; }
         }
         __syncthreads();
-        mark(3);
+        mark(7);
 
         // ------------------------------------------------------------ P3
         if constexpr (!ROUTED) {
@@ -869,7 +858,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             }
         }
         __syncthreads();
-        mark(4);
+        mark(8);
 
         // ------------------------------------------------------------ P4
         // per (interface, flux component): full WENO -> F_i + sum_m R(r,m) F^_m
@@ -890,15 +879,14 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 for (int m = 0; m < 7; ++m) acc += sR[(m * 7 + r) * NI + i] * sFs[m * NI + i];
                 dF = (double)acc + F2;
             } else {
-                R amx = R(0);
                 R dFk[5], dqk[5];
 #pragma unroll
-                for (int k = 0; k < 6; ++k) {
+                for (int k = 0; k < 5; ++k) {
                     const int cc = l * C + f + k;
-                    amx = fmax(amx, fmax(fabs(sA[0 * NLC + cc]), fabs(sA[6 * NLC + cc])));
-                    if (k < 5) { dFk[k] = sD[cc * 14 + r]; dqk[k] = sD[cc * 14 + 7 + r]; }
+                    dFk[k] = sD[cc * 14 + r];
+                    dqk[k] = sD[cc * 14 + 7 + r];
                 }
-                dF = (double)linear_flux_d<R>(dFk, dqk, amx) + F2;
+                dF = (double)linear_flux_d<R>(dFk, dqk, sAmx[i]) + F2;
             }
             sdF[r * NI + i] = dF;
             const int iface = c0 + f;   // global interface index, face at padded iface + 2
@@ -927,7 +915,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 if (valid && r == 0 && (f < T || iface == n)) {
                     const long long o = line_off(l) + (long long)(iface + 2) * sstride;
                     if constexpr (ROUTED) {
-                        a.route_next[o] = (unsigned char)(full ? 1 : 0);
+                        if constexpr (MODE == 2) a.route_next[o] = (unsigned char)(full ? 1 : 0);
                         atomicAdd(&s_cnt[full ? 0 : 1], 1u);
                     }
                     if constexpr (MODE == 3) {
@@ -954,9 +942,10 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             if (tid == 0) {
                 atomicAdd(&a.route_count[0], (unsigned long long)s_cnt[0]);
                 atomicAdd(&a.route_count[1], (unsigned long long)s_cnt[1]);
+
             }
         }
-        mark(5);
+        mark(9);
 
         // ------------------------------------------------------------ P5
         {
@@ -994,7 +983,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 pend_bits |= 4u;
             }
         }
-        mark(6);
+        mark(10);
         buf ^= 1;
     }   // tile loop
 }

@@ -104,6 +104,7 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     a.ct4 = c.p.ct_avg == 4;
     const bool mixed = c.precision == HOW_PREC_MIXED;
     const int mode = c.route_mode;
+    if (mode == 1) launch_route(c, dir, a.qprev, a.route_prev, a.route_next);
     // instantiations: {fp64, mixed} x {plain, learned, guard-only}; label
     // collection runs the FP64 method
 #define HOW_SWEEP_CASES(D)                                                                              \

@@ -125,6 +125,7 @@ def _load():
         "how_router_set_weights": ([V, F, ctypes.c_int], ctypes.c_int),
         "how_router_configure": ([V, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float], ctypes.c_int),
         "how_router_stats": ([V, U64P, U64P, ctypes.c_int], ctypes.c_int),
+        "how_router_stats4": ([V, U64P, U64P, U64P, U64P, ctypes.c_int], ctypes.c_int),
         "how_collect_begin": ([V, ctypes.c_uint, ctypes.c_uint], ctypes.c_int),
         "how_collect_end": ([V, F, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)], ctypes.c_int),
         "how_router_train": ([F, F, F, ctypes.c_long, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float,
@@ -340,8 +341,8 @@ class Domain:
 
     def sweep_phase_profile(self, direction: int, dt: float):
         """Mean cycles per block of each sweep phase (instrumentation)."""
-        out = np.zeros(8)
-        _check(_lib.how_sweep_phase_profile(self._h, direction, dt, _dptr(out), 8))
+        out = np.zeros(12)
+        _check(_lib.how_sweep_phase_profile(self._h, direction, dt, _dptr(out), 12))
         return out
 
     def set_precision(self, mode):
@@ -362,11 +363,13 @@ class Domain:
             _check(_lib.how_router_set_weights(self._h, _fptr(w), w.size))
         _check(_lib.how_router_configure(self._h, m, threshold, guard_jump, guard_floor))
 
-    def router_stats(self, reset=False):
-        """(full, cheap) interface counts since the last reset."""
-        a, b = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
-        _check(_lib.how_router_stats(self._h, ctypes.byref(a), ctypes.byref(b), int(reset)))
-        return a.value, b.value
+    def router_stats(self, reset=False, groups=False):
+        """(full, cheap) interface counts since the last reset; with groups=True
+        also the 16-interface groups inferred on the tensor cores and the flat
+        groups that used the precomputed logit."""
+        v = [ctypes.c_ulonglong(0) for _ in range(4)]
+        _check(_lib.how_router_stats4(self._h, *(ctypes.byref(x) for x in v), int(reset)))
+        return tuple(x.value for x in v) if groups else (v[0].value, v[1].value)
 
     def collect_begin(self, capacity, every=1):
         _check(_lib.how_collect_begin(self._h, capacity, every))

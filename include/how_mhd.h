@@ -166,8 +166,10 @@ int how_set_kernel_timing(how_ctx* ctx, int on);
 int how_get_kernel_timing(how_ctx* ctx, double* total_ms, long* launches);
 /* Mean cycles per thread block of each phase of one stage-1 sweep (the
  * how_sweep semantics) -- instrumentation, no reference counterpart.
- * out[0..6] = phases (load, primitives, differences+scalars, eigenvector
- * rows, projection+WENO, back-projection+CT, update); out[7] = blocks. */
+ * out[0..10] = phases (load, primitives, cell differences, routing features,
+ * routing network, routing decision, eigen-system scalars, eigenvector rows,
+ * projection+WENO, back-projection+CT, update); out[11] = tiles.  A phase a
+ * launch does not have adds nothing. */
 int how_sweep_phase_profile(how_ctx* ctx, int dir, double dt, double* out, int nout);
 /* ------------------------------------------------------ batched ensembles */
 /* No counterpart in the reference (which runs one domain per job).  Many
@@ -214,6 +216,10 @@ int how_router_set_weights(how_ctx* ctx, const float* w, int n);
 /* mode 0 off, 1 network + guard, 2 guard only; full WENO when logit > threshold */
 int how_router_configure(how_ctx* ctx, int mode, float threshold, float guard_jump, float guard_floor);
 int how_router_stats(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap, int reset);
+/* ... plus the 16-interface groups whose logits came from the tensor cores and
+ * those taken from the precomputed logit of a uniform stencil */
+int how_router_stats4(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap,
+                      unsigned long long* mma_groups, unsigned long long* flat_groups, int reset);
 /* Label collection from the plain FP64 method (records of 8 floats). */
 int how_collect_begin(how_ctx* ctx, unsigned int capacity, unsigned int every);
 int how_collect_end(how_ctx* ctx, float* out, unsigned int cap, unsigned int* n);

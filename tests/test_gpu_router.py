@@ -149,3 +149,45 @@ def test_routed_all_linear_converges_to_plain_on_alfven():
         assert np.isfinite(out[1]).all()
         diffs.append(np.abs(out[1][5] - out[0][5]).mean())
     assert diffs[1] > 0 and diffs[0] / diffs[1] >= 16.0, diffs
+
+
+def _blast_final(n, tend, precision, router=None, mode="learned"):
+    import how_mhd as hm
+    p = hm.make_parameters(nx=n, ny=n, nz=n, nt=1, tend=tend, gam=5.0 / 3.0, cour=0.4, problem="blast3d_b",
+                           rhomin=1e-6, pgmin=1e-6, precision=precision)
+    with hm.Domain(p) as d:
+        d.init_problem()
+        if router is not None:
+            w, thr = router
+            d.set_router(w, mode, threshold=thr)
+        d.run(0.0, -1)
+        st = d.router_stats() if router is not None else (0, 0)
+        return active(d.get_state(0), n, n, n)[0].copy(), st
+
+
+def test_trained_router_accuracy_and_ablation():
+    """The built-in network on the magnetised blast (64^3 to t = 0.2): mixed
+    precision + learned routing stays within density L1 1e-5 of plain FP64
+    while sending most interfaces to the linear flux; the same routing without
+    the network (guard only) is far less accurate -- what the network adds."""
+    import how_mhd as hm
+    w, thr = hm.default_router()
+    ref, _ = _blast_final(64, 0.2, "fp64")
+    learned, (f1, c1) = _blast_final(64, 0.2, "mixed", (w, thr), "learned")
+    guard, (f2, c2) = _blast_final(64, 0.2, "mixed", (w, thr), "guard")
+    l1 = lambda a: float(np.abs(a - ref).sum() / np.abs(ref).sum())
+    e_learned, e_guard = l1(learned), l1(guard)
+    assert e_learned <= 1e-5, e_learned
+    assert f1 / (f1 + c1) < 0.5, (f1, c1)
+    assert e_guard >= 10.0 * e_learned and e_guard > 1e-5, (e_guard, e_learned)
+
+
+def test_router_on_key_uses_builtin_network():
+    import how_mhd as hm
+    p = hm.make_parameters(nx=32, ny=32, nz=32, nt=1, tend=100.0, gam=5.0 / 3.0, cour=0.4, problem="blast3d_b",
+                           rhomin=1e-6, pgmin=1e-6, precision="mixed", router="on")
+    with hm.Domain(p) as d:
+        d.init_problem()
+        d.run(0.0, 3)
+        full, cheap, mma, flat = d.router_stats(groups=True)
+    assert full > 0 and cheap > 0 and mma + flat > 0
