@@ -534,7 +534,7 @@ def bench_ensemble(args):
                    "members": len(members), "zones": zones, "timing": "host clock around synchronised runs"},
         "one_by_one": {"value": world * zones * args.steps / seq_s, "unit": UNIT, "seconds": seq_s},
         "speedup_vs_one_by_one": seq_s / ens_s,
-        "tile_shapes": {d: hm.Ensemble.shape_info(d, s) for d, s in zip("xyz", shapes)},
+        "tile_shapes": {name: hm.Ensemble.shape_info(d, s) for d, (name, s) in enumerate(zip("xyz", shapes))},
         "autotune_sweep_ms": sweep_ms.tolist(),
         "graph_launches": launches,
     }

@@ -38,7 +38,8 @@ constexpr int kRouteThreads = 256;
 
 // Routing values of one cell: floored density and pressure (the sweep's
 // primit floors, src/ssprk.cpp:479-512), |B|, |v| and the fast speed along
-// the sweep normal, in the sweep's arithmetic order.
+// the sweep normal.  Density, velocity and pressure in FP64 (one division);
+// the square roots of the fast speed in FP32, which is all the features keep.
 __device__ __forceinline__ StencilCell route_cell(const double* q, long long fs, long long c, int dir, double gam,
                                                   double rhomin, double pgmin) {
     const double DD = q[c];
@@ -47,46 +48,67 @@ __device__ __forceinline__ StencilCell route_cell(const double* q, long long fs,
     const double Bx = q[route_perm(dir, 4) * fs + c], By = q[route_perm(dir, 5) * fs + c];
     const double Bz = q[route_perm(dir, 6) * fs + c];
     const double EE = q[7 * fs + c];
-    double rho = DD;
-    double irho = 1.0 / rho;
-    const double vx = Mx * irho, vy = My * irho, vz = Mz * irho;
+    const double irho0 = 1.0 / DD;
+    const double vx = Mx * irho0, vy = My * irho0, vz = Mz * irho0;
     const double vv2 = vx * vx + vy * vy + vz * vz;
     const double BB2 = Bx * Bx + By * By + Bz * Bz;
-    double pg = (gam - 1.0) * (EE - 0.5 * (rho * vv2 + BB2));
-    if (rho < rhomin || pg < pgmin) {
-        rho = fmax(rhomin, rho);
-        pg = fmax(pgmin, pg);
-        irho = 1.0 / rho;
-    }
-    const double bbn2 = BB2 * irho;
-    const double bnx2 = Bx * Bx * irho;
-    const double cs2 = fmax(0.0, gam * fabs(pg * irho));
-    const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
-    const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
-    return StencilCell{(float)rho, (float)pg, sqrtf((float)BB2), sqrtf((float)vv2), (float)lf};
+    const double pg = fmax(pgmin, (gam - 1.0) * (EE - 0.5 * (DD * vv2 + BB2)));
+    const double rho = fmax(rhomin, DD);
+    const float irho = 1.0f / (float)rho;
+    const float bbn2 = (float)BB2 * irho, bnx2 = (float)(Bx * Bx) * irho;
+    const float cs2 = fmaxf(0.0f, (float)gam * fabsf((float)pg * irho));
+    const float root = sqrtf(fmaxf(0.0f, (bbn2 + cs2) * (bbn2 + cs2) - 4.0f * bnx2 * cs2));
+    const float lf = sqrtf(fmaxf(0.0f, 0.5f * (bbn2 + cs2 + root)));
+    return StencilCell{(float)rho, (float)pg, sqrtf((float)BB2), sqrtf((float)vv2), lf};
 }
 
-// Each thread walks one segment of kSeg interfaces of one line along the
-// sweep direction with a sliding window of its 6 stencil cells, so every cell's
-// routing values are formed once per segment (kSeg + 5 cells for kSeg faces).
-// Lanes of a warp hold consecutive lines (x-adjacent for the y and z sweeps:
-// coalesced loads), and at every step the warp's 32 interfaces are two 16-row
-// groups of the network.
-constexpr int kSeg = 32;
+// A warp's 32 interfaces as two 16-row groups of the network: features to the
+// BF16 operand rows, the tensor-core logits (or the flat logit of a group of
+// uniform stencils), the decision.  Every lane of the warp calls this.
+struct RouteShared {
+    RouterSmem rs;
+    __align__(16) __nv_bfloat16 X[kRouteThreads / 32][32][16];
+    float lg[kRouteThreads / 32][32];
+    float flat_logit[2];
+    unsigned int cnt[2];
+};
 
-template <int DIR>
-__global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__ RouteArgs a) {
-    __shared__ RouterSmem rs;
-    __shared__ __align__(16) __nv_bfloat16 X[kRouteThreads / 32][32][16];
-    __shared__ float lg[kRouteThreads / 32][32];
-    __shared__ float flat_logit[2];
-    __shared__ unsigned int cnt[2];
+__device__ __forceinline__ void route_decide(RouteShared& S, const RouteArgs& a, int warp, int lane,
+                                             const float* ft, bool flat, bool guard, bool live, long long face) {
+    uint4 v0;
+    v0.x = pack_bf16(ft[0], ft[1]); v0.y = pack_bf16(ft[2], ft[3]);
+    v0.z = pack_bf16(ft[4], ft[5]); v0.w = 0u;
+    reinterpret_cast<uint4*>(&S.X[warp][lane][0])[0] = v0;
+    reinterpret_cast<uint4*>(&S.X[warp][lane][0])[1] = make_uint4(0u, 0u, 0u, 0u);
+    const int code = flat ? 1 + (ft[5] > 0.5f ? 1 : 0) : 0;
+    __syncwarp();
+    float logit = 0.0f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const unsigned int nonflat = __ballot_sync(0xffffffffu, code == 0);
+        const unsigned int half = h == 0 ? 0x0000ffffu : 0xffff0000u;
+        if ((nonflat & half) == 0u) {
+            if ((lane >> 4) == h) logit = S.flat_logit[code - 1];
+            if (lane == 0) atomicAdd(&S.cnt[1], 1u);
+        } else {
+            router_mma_16rows(&S.rs, S.X[warp] + 16 * h, S.lg[warp] + 16 * h);
+            __syncwarp();
+            if ((lane >> 4) == h) logit = S.lg[warp][lane];
+            if (lane == 0) atomicAdd(&S.cnt[0], 1u);
+        }
+    }
+    if (live) a.next[face] = (guard || logit > a.thr) ? 1 : 0;
+    __syncwarp();
+}
+
+// The network in shared memory and the logits of a uniform stencil with prior
+// 0 and 1, through the same code as every face (runtime cell values).
+__device__ __forceinline__ void route_setup(RouteShared& S, const RouteArgs& a) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    router_load_smem(&rs, a.w, tid, blockDim.x);
-    if (tid < 2) cnt[tid] = 0u;
+    router_load_smem(&S.rs, a.w, tid, blockDim.x);
+    if (tid < 2) S.cnt[tid] = 0u;
     __syncthreads();
     if (warp == 0) {
-        // logits of a uniform stencil with prior 0 and 1, through the same code
         StencilCell sc[6];
         const float u = (float)a.gam;
         for (int k = 0; k < 6; ++k) sc[k] = StencilCell{u, u, u, u, u};
@@ -95,20 +117,87 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__
         router_features(sc, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, ff, &flat);
         for (int e = lane; e < 256; e += 32) {
             const int r = e / 16, k = e % 16;
-            X[0][r][k] = __float2bfloat16_rn(k < 5 ? ff[k] : k == 5 ? (float)(r & 1) : 0.0f);
+            S.X[0][r][k] = __float2bfloat16_rn(k < 5 ? ff[k] : k == 5 ? (float)(r & 1) : 0.0f);
         }
         __syncwarp();
-        router_mma_16rows(&rs, X[0], lg[0]);
+        router_mma_16rows(&S.rs, S.X[0], S.lg[0]);
         __syncwarp();
-        if (lane < 2) flat_logit[lane] = lg[0][lane];
+        if (lane < 2) S.flat_logit[lane] = S.lg[0][lane];
     }
     __syncthreads();
+}
 
+__device__ __forceinline__ void route_finish(RouteShared& S, const RouteArgs& a) {
+    __syncthreads();
+    if (threadIdx.x == 0 && a.groups) {
+        atomicAdd(&a.groups[0], (unsigned long long)S.cnt[0]);
+        atomicAdd(&a.groups[1], (unsigned long long)S.cnt[1]);
+    }
+}
+
+// x sweeps: a warp takes 32 consecutive faces of one line; its lanes form
+// the values of 37 consecutive cells (coalesced along x) into shared memory
+// and each lane reads its face's 6.
+__global__ void __launch_bounds__(kRouteThreads) k_route_x(const __grid_constant__ RouteArgs a) {
+    __shared__ RouteShared S;
+    __shared__ float cv[kRouteThreads / 32][37][5];
+    route_setup(S, a);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const Grid& g = a.g;
-    const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
-    const long long stride = DIR == 0 ? 1ll : DIR == 1 ? (long long)g.pitch : (long long)g.pitch * g.P1;
-    // lines: DIR 0 (j, k); DIR 1 (i, k); DIR 2 (i, j) -- the faster index first
-    const int la = DIR == 0 ? g.ny : g.nx;
+    const int n = g.nx;
+    const int nseg = (n + 1 + 31) / 32;
+    const long long nwork = (long long)g.ny * g.nz * nseg;   // (segment, line)
+    const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long wi = (long long)blockIdx.x * (blockDim.x >> 5) + warp; wi < nwork; wi += wstride) {
+        const int seg = (int)(wi % nseg);
+        const long long ln = wi / nseg;
+        const long long line = g.idx(0, 3 + (int)(ln % g.ny), 3 + (int)(ln / g.ny));
+        const int f0 = seg * 32;
+        for (int k = lane; k < 37; k += 32) {
+            const int s = f0 + k;   // padded cell index
+            StencilCell v = StencilCell{0.f, 0.f, 0.f, 0.f, 0.f};
+            if (s <= n + 5) v = route_cell(a.q, g.fs, line + s, 0, a.gam, a.rhomin, a.pgmin);
+            cv[warp][k][0] = v.rho; cv[warp][k][1] = v.p; cv[warp][k][2] = v.bmag;
+            cv[warp][k][3] = v.vmag; cv[warp][k][4] = v.cf;
+        }
+        __syncwarp();
+        const int iface = f0 + lane;
+        const bool live = iface <= n;
+        float ft[kRouterNF] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        bool flat = true, guard = false;
+        const long long face = line + iface + 2;
+        if (live) {
+            StencilCell sc[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                sc[k] = StencilCell{cv[warp][lane + k][0], cv[warp][lane + k][1], cv[warp][lane + k][2],
+                                    cv[warp][lane + k][3], cv[warp][lane + k][4]};
+            guard = router_features(sc, (float)a.prev[face], (float)a.rhomin, (float)a.pgmin, a.guard_jump,
+                                    a.guard_floor, ft, &flat);
+        }
+        route_decide(S, a, warp, lane, ft, flat, guard, live, face);
+    }
+    route_finish(S, a);
+}
+
+// y/z sweeps: each thread walks one segment of kSeg interfaces of one line
+// along the sweep direction with a sliding window of its 6 stencil cells, so
+// every cell's routing values are formed once per segment (kSeg + 5 cells for
+// kSeg faces); lanes of a warp hold x-adjacent lines (coalesced loads), and at
+// every step the warp's 32 interfaces are two 16-row groups of the network.
+constexpr int kSeg = 32;
+
+// y and z sweeps (see above): sliding windows along the sweep direction.
+template <int DIR>
+__global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__ RouteArgs a) {
+    __shared__ RouteShared S;
+    route_setup(S, a);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Grid& g = a.g;
+    const int n = DIR == 1 ? g.ny : g.nz;
+    const long long stride = DIR == 1 ? (long long)g.pitch : (long long)g.pitch * g.P1;
+    // lines: DIR 1 (i, k); DIR 2 (i, j) -- i fastest
+    const int la = g.nx;
     const int lb = DIR == 2 ? g.ny : g.nz;
     const long long nlines = (long long)la * lb;
     const int nseg = (n + 1 + kSeg - 1) / kSeg;
@@ -122,7 +211,7 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__
             const long long ln = widx % nlines;
             f0 = (int)(widx / nlines) * kSeg;
             const int ia = (int)(ln % la), ib = (int)(ln / la);
-            line = DIR == 0 ? g.idx(0, 3 + ia, 3 + ib) : DIR == 1 ? g.idx(3 + ia, 0, 3 + ib) : g.idx(3 + ia, 3 + ib, 0);
+            line = DIR == 1 ? g.idx(3 + ia, 0, 3 + ib) : g.idx(3 + ia, 3 + ib, 0);
         }
         // window: stencil cells f .. f+5 of face f (padded cells)
         StencilCell win[6];
@@ -139,44 +228,16 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__
             const long long face = line + (long long)(iface + 2) * stride;
             if (live) {
                 win[5] = route_cell(a.q, g.fs, line + (long long)(iface + 5) * stride, DIR, a.gam, a.rhomin, a.pgmin);
-                const float prior = (float)a.prev[face];
-                guard = router_features(win, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump, a.guard_floor, ft,
-                                        &flat);
+                guard = router_features(win, (float)a.prev[face], (float)a.rhomin, (float)a.pgmin, a.guard_jump,
+                                        a.guard_floor, ft, &flat);
 #pragma unroll
                 for (int k = 0; k < 5; ++k) win[k] = win[k + 1];
             }
-            uint4 v0;
-            v0.x = pack_bf16(ft[0], ft[1]); v0.y = pack_bf16(ft[2], ft[3]);
-            v0.z = pack_bf16(ft[4], ft[5]); v0.w = 0u;
-            reinterpret_cast<uint4*>(&X[warp][lane][0])[0] = v0;
-            reinterpret_cast<uint4*>(&X[warp][lane][0])[1] = make_uint4(0u, 0u, 0u, 0u);
-            const int code = flat ? 1 + (ft[5] > 0.5f ? 1 : 0) : 0;
             // every lane of the warp reaches here kSeg times (uniform trip count)
-            __syncwarp();
-            float logit = 0.0f;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const unsigned int nonflat = __ballot_sync(0xffffffffu, code == 0);
-                const unsigned int half = h == 0 ? 0x0000ffffu : 0xffff0000u;
-                if ((nonflat & half) == 0u) {
-                    if ((lane >> 4) == h) logit = flat_logit[code - 1];
-                    if (lane == 0) atomicAdd(&cnt[1], 1u);
-                } else {
-                    router_mma_16rows(&rs, X[warp] + 16 * h, lg[warp] + 16 * h);
-                    __syncwarp();
-                    if ((lane >> 4) == h) logit = lg[warp][lane];
-                    if (lane == 0) atomicAdd(&cnt[0], 1u);
-                }
-            }
-            if (live) a.next[face] = (guard || logit > a.thr) ? 1 : 0;
-            __syncwarp();
+            route_decide(S, a, warp, lane, ft, flat, guard, live, face);
         }
     }
-    __syncthreads();
-    if (tid == 0 && a.groups) {
-        atomicAdd(&a.groups[0], (unsigned long long)cnt[0]);
-        atomicAdd(&a.groups[1], (unsigned long long)cnt[1]);
-    }
+    route_finish(S, a);
 }
 
 }  // namespace
@@ -200,13 +261,14 @@ void launch_route(Ctx& c, int dir, const double* q, const unsigned char* prev, u
     const int n = dir == 0 ? g.nx : dir == 1 ? g.ny : g.nz;
     const long long nlines = dir == 0 ? (long long)g.ny * g.nz : dir == 1 ? (long long)g.nx * g.nz
                                                                         : (long long)g.nx * g.ny;
-    const long long nwork = nlines * ((n + 1 + kSeg - 1) / kSeg);
+    // x: one warp per (32-face segment, line); y/z: one thread per (kSeg-face segment, line)
+    const long long nwork = dir == 0 ? nlines * ((n + 1 + 31) / 32) * 32 : nlines * ((n + 1 + kSeg - 1) / kSeg);
     long long blocks = (nwork + kRouteThreads - 1) / kRouteThreads;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
     if (blocks > (long long)nsm * 8) blocks = (long long)nsm * 8;
     if (blocks < 1) blocks = 1;
-    if (dir == 0) k_route<0><<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
+    if (dir == 0) k_route_x<<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
     else if (dir == 1) k_route<1><<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
     else k_route<2><<<(unsigned)blocks, kRouteThreads, 0, c.stream>>>(a);
     ++c.launches;

@@ -440,14 +440,20 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             }
         }
         // MODE 1: this tile's routing decisions (formed by the routing pass),
-        // loaded now so their latency hides behind P1
-        int pre_dec = 0;
+        // fetched now by asynchronous 4-byte copies of the aligned words that
+        // hold them, so their latency hides behind P1
+        int dec_shift = -1;   // byte of the word, -1: no valid face
         if constexpr (MODE == 1) {
             if (tid < NLF) {
                 const int l = tid / F, f = tid % F;
                 const int iface = c0 + f;
-                if (line_ok(l) && iface <= n) pre_dec = a.route_next[line_off(l) + (long long)(iface + 2) * sstride];
+                if (line_ok(l) && iface <= n) {
+                    const unsigned char* src = a.route_next + line_off(l) + (long long)(iface + 2) * sstride;
+                    dec_shift = (int)(reinterpret_cast<uintptr_t>(src) & 3u);
+                    cp_async4(&sDec[tid], reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3)));
+                }
             }
+            cp_async_commit();
         }
         mark(0);
 
@@ -556,8 +562,9 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 // decisions of the learned router, formed for the whole sweep by
                 // the routing pass (route_prepass.cu) before this launch
                 static_assert(NLF <= NT, "one decision per thread");
+                cp_async_wait_all();
                 if (tid < NLF) {
-                    sDec[tid] = pre_dec;
+                    sDec[tid] = dec_shift < 0 ? 0 : (int)((((unsigned int)sDec[tid]) >> (8 * dec_shift)) & 0xffu);
                     row_amx(tid);
                 }
                 __syncthreads();
