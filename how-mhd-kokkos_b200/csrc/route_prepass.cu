@@ -80,15 +80,17 @@ __device__ __forceinline__ void route_decide(RouteShared& S, const RouteArgs& a,
     v0.z = pack_bf16(ft[4], ft[5]); v0.w = 0u;
     reinterpret_cast<uint4*>(&S.X[warp][lane][0])[0] = v0;
     reinterpret_cast<uint4*>(&S.X[warp][lane][0])[1] = make_uint4(0u, 0u, 0u, 0u);
-    const int code = flat ? 1 + (ft[5] > 0.5f ? 1 : 0) : 0;
+    // 0: needs the network; 1 + prior: uniform stencil (flat logit);
+    // 3: guarded or no face (decided without a logit)
+    const int code = (guard || !live) ? 3 : flat ? 1 + (ft[5] > 0.5f ? 1 : 0) : 0;
     __syncwarp();
     float logit = 0.0f;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-        const unsigned int nonflat = __ballot_sync(0xffffffffu, code == 0);
+        const unsigned int needs = __ballot_sync(0xffffffffu, code == 0);
         const unsigned int half = h == 0 ? 0x0000ffffu : 0xffff0000u;
-        if ((nonflat & half) == 0u) {
-            if ((lane >> 4) == h) logit = S.flat_logit[code - 1];
+        if ((needs & half) == 0u) {
+            if ((lane >> 4) == h && code < 3) logit = S.flat_logit[code - 1];
             if (lane == 0) atomicAdd(&S.cnt[1], 1u);
         } else {
             router_mma_16rows(&S.rs, S.X[warp] + 16 * h, S.lg[warp] + 16 * h);

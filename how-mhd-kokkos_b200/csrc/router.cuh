@@ -50,8 +50,10 @@ __device__ __forceinline__ float tanh_fast(float x) {
 }
 
 __device__ __forceinline__ float gelu_fast(float x) {
-    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-    return 0.5f * x * (1.0f + tanh_fast(u));
+    // sqrt(2/pi) (x + 0.044715 x^3) = x (0.79788456 + 0.03567741 x^2)
+    const float u = x * fmaf(0.0356774081363001f, x * x, 0.7978845608028654f);
+    const float hx = 0.5f * x;
+    return fmaf(hx, tanh_fast(u), hx);
 }
 
 // Features from the stencil's cell values; returns the guard decision.

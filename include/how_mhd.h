@@ -217,7 +217,8 @@ int how_router_set_weights(how_ctx* ctx, const float* w, int n);
 int how_router_configure(how_ctx* ctx, int mode, float threshold, float guard_jump, float guard_floor);
 int how_router_stats(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap, int reset);
 /* ... plus the 16-interface groups whose logits came from the tensor cores and
- * those taken from the precomputed logit of a uniform stencil */
+ * those that needed no tensor-core pass (every stencil uniform -- the
+ * precomputed flat logit -- or guarded) */
 int how_router_stats4(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap,
                       unsigned long long* mma_groups, unsigned long long* flat_groups, int reset);
 /* Label collection from the plain FP64 method (records of 8 floats). */
