@@ -411,9 +411,26 @@ def bench_ours(args):
                 "max_div_b": div4_max(bf, n, pf.dx),
                 "router_threshold": thr, "gpu_launches": flaunch,
                 "sweep_avg_ms": fsw_ms / max(fsw_n, 1),
-                "note": "same start state and step count as the plain FP64 leg; L1 over active cells",
+                "note": "same start state and step count as the plain FP64 leg; L1 over active cells; the network decides once per step, the guard every stage",
             }
             del qf, bf
+        domf.close()
+        # the same form with the network's decisions formed at every stage
+        pf, domf = make_domain("mixed", "on")
+        domf.set_router_refresh(1)
+        domf.router_stats(reset=True)
+        sms, _, _, _, _ = timed_leg(domf, False)
+        full5, cheap5 = domf.router_stats()
+        if rank == 0:
+            qf = domf.get_state(0)
+            rf = qf[0, 3:n + 3, 3:n + 3, 3:n + 3]
+            v5 = replica_value(world, n ** 3, args.steps, sms)
+            fast["decisions_every_stage"] = {
+                "value": v5, "ms_per_step": sms / args.steps, "speedup_vs_plain_fp64": v5 / value,
+                "full_weno_fraction": full5 / max(full5 + cheap5, 1),
+                "l1_rho_vs_fp64": float(np.abs(rf - rho64).sum() / np.abs(rho64).sum()),
+            }
+            del qf
         domf.close()
 
     if world > 1:
@@ -556,15 +573,17 @@ def bench_accuracy(args):
     n = args.n
     s = slice(3, n + 3)
     w, thr = hm.default_router()
-    forms = [("fp64", "fp64", None), ("mixed", "mixed", None), ("mixed+learned", "mixed", "learned"),
-             ("mixed+guard", "mixed", "guard")]
+    forms = [("fp64", "fp64", None, 5), ("mixed", "mixed", None, 5), ("mixed+learned", "mixed", "learned", 5),
+             ("mixed+learned, decisions every stage", "mixed", "learned", 1),
+             ("mixed+guard", "mixed", "guard", 5)]
     out, ref = {}, None
-    for name, prec, mode in forms:
+    for name, prec, mode, refresh in forms:
         p = hm.read_parameters(workload_text(n, prec, tend=args.tend))
         with hm.Domain(p) as d:
             d.init_problem()
             if mode:
                 d.set_router(w, mode, threshold=thr)
+                d.set_router_refresh(refresh)
             d.sync()
             t0 = time.perf_counter()
             t, steps, _ = d.run(0.0, -1)

@@ -73,6 +73,7 @@ int encode_tensor_map_4d(CUtensorMap* map, const void* base, const uint64_t dims
 // q(iw-1) already had its ghosts filled at the end of the previous stage.
 static void run_stage(Ctx& c, int iw) {
     const Grid& g = c.g;
+    c.cur_stage = iw;
     const RKCoeff k = rk_coeff(iw);
     const double c4 = iw == 5 ? k.k4 / k.k1 : 0.0;
     const double c5 = iw == 5 ? k.k5 / k.k1 : 0.0;
@@ -382,6 +383,7 @@ int how_sweep(how_ctx* c, int dir, double dt) {
     const int n = dir == 0 ? c->g.nx : dir == 1 ? c->g.ny : c->g.nz;
     if (n <= 1) { set_error("no sweep along an axis with one cell"); return HOW_ERR_ARG; }
     if ((rc = upload_dt(c, dt))) return rc;
+    c->cur_stage = 1;
     // stage 1: copy_stage(q, 1, 0) then the sweep (src/ssprk.cpp:1288, 1306-1317)
     launch_copy_fields(*c, c->q[1], c->q[0], 8);
     const RKCoeff k = rk_coeff(1);

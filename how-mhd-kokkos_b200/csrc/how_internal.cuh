@@ -139,6 +139,8 @@ struct Ctx {
     unsigned int* collect_n = nullptr;
     unsigned int collect_cap = 0, collect_every = 1;
     float route_thr = 0.0f, guard_jump = 0.25f, guard_floor = 100.0f;
+    int route_refresh = 5;                // learned routing: fresh decisions every this many stages (1..5)
+    int cur_stage = 1;                    // SSPRK stage being launched (1..5)
 };
 
 // ---- kernels / launchers (defined in the .cu files) ------------------------

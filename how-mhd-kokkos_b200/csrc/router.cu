@@ -298,6 +298,16 @@ int how_router_configure(how_ctx* c, int mode, float threshold, float guard_jump
     return HOW_OK;
 }
 
+// Learned routing forms the network's decisions every `stages` stages (5:
+// once per step, at its first stage -- the default; 1: every stage); in
+// between the sweeps reuse them, and re-evaluate the hard guard on each
+// stage's own state.
+int how_router_set_refresh(how_ctx* c, int stages) {
+    if (!c || stages < 1 || stages > 5) { set_error("router refresh: 1..5 stages"); return HOW_ERR_ARG; }
+    c->route_refresh = stages;
+    return HOW_OK;
+}
+
 // Interfaces (active faces) sent to full WENO and to the linear flux since
 // the last reset.
 int how_router_stats4(how_ctx* c, unsigned long long* full, unsigned long long* cheap,

@@ -84,9 +84,31 @@ __device__ __forceinline__ bool router_features(const StencilCell* s, float prio
     feat[4] = log10f(1e-6f + dcf / fmaxf(mincf, tiny));
     feat[5] = prior;
     *flat = drho == 0.0f && dp == 0.0f && db == 0.0f && dv == 0.0f && dcf == 0.0f;
-    const bool bad = !(jr == jr) || !(jp == jp);   // NaN anywhere: full method
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sum += s[k].rho + s[k].p;
+    const bool bad = !(sum == sum) || !(jr == jr) || !(jp == jp);   // NaN anywhere: full method
     return bad || jr > guard_jump || jp > guard_jump || minrho < guard_floor * rhomin ||
            minp < guard_floor * pgmin;
+}
+
+// The guard from 6 consecutive densities and pressures, without divisions
+// (jump > guard_jump * min is the same test; a NaN fails every comparison).
+__device__ __forceinline__ bool router_guard_rp(const float* rho, const float* p, float rhomin, float pgmin,
+                                                float guard_jump, float guard_floor) {
+    float minrho = rho[0], minp = p[0], drho = 0.f, dp = 0.f, sum = rho[0] + p[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k) {
+        minrho = fminf(minrho, rho[k]);
+        minp = fminf(minp, p[k]);
+        drho = fmaxf(drho, fabsf(rho[k] - rho[k - 1]));
+        dp = fmaxf(dp, fabsf(p[k] - p[k - 1]));
+        sum += rho[k] + p[k];   // NaN anywhere makes the sum NaN (fminf/fmaxf drop it)
+    }
+    const float tiny = 1e-30f;
+    const bool ok = sum == sum && drho <= guard_jump * fmaxf(minrho, tiny) && dp <= guard_jump * fmaxf(minp, tiny) &&
+                    minrho >= guard_floor * rhomin && minp >= guard_floor * pgmin;
+    return !ok;
 }
 
 // FP32 reference of the network (training, checks): w packed as RouterLayout.

@@ -111,7 +111,8 @@ struct Tile {
     static constexpr int bFt = bDev + align_up(4 * NLF, 16);      // [NLF][6] float
     static constexpr int bAmx = bFt + align_up(4 * 6 * NLF, 16);  // [NLF] R: linear-flux LF speed
     static constexpr int bCF = bAmx + align_up((int)sizeof(R) * NLF, 16);   // [5][NLC] float cell features
-    static constexpr int bEnd = bCF + align_up(4 * 5 * NLC, 16);
+    static constexpr int bDecW = bCF + align_up(4 * 5 * NLC, 16);  // [NL][F+2] int: fetched decisions
+    static constexpr int bEnd = bDecW + align_up(4 * NL * (F + 2), 16);
     static constexpr size_t bytes_plain = (size_t)bB + 3 * 8;
     static constexpr size_t bytes_route = (size_t)bEnd;
     static constexpr uint32_t in_bytes = 8u * NQ;
@@ -255,6 +256,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     float* sFt = reinterpret_cast<float*>(sm + TL::bFt);        // features (collect)
     R* sAmx = reinterpret_cast<R*>(sm + TL::bAmx);              // per interface: max |lambda_0|, |lambda_6|
     float* sCF = reinterpret_cast<float*>(sm + TL::bCF);        // per cell: rho, p, |B|, |v|, c_f (routing)
+    int* sDecW = reinterpret_cast<int*>(sm + TL::bDecW);        // MODE 1: fetched decisions (words, then bytes)
     __shared__ int s_nfull;
     __shared__ unsigned int s_cnt[2];   // full, cheap interfaces
 
@@ -315,8 +317,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         return t;
     };
     const int tid = threadIdx.x;
+    // the thread that issues and tracks the tile copies: the block's last,
+    // whose warp has the least P1 work, so issuing does not delay P1
+    const bool issuer = tid == NT - 1;
 
-    if (tid == 0) {
+    if (issuer) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init(&bars[2], 1);
@@ -324,7 +329,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     }
     __syncthreads();
 
-    // TMA loads (thread 0 only): the raw tile of `tile` into buffer b
+    // TMA loads (the issuer only): the raw tile of `tile` into buffer b
     // (which == 0) or its update operand (which == 1).
     auto issue = [&](long long gtile, int which, int b) -> bool {
         long long tile;
@@ -364,16 +369,16 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     long long tile = advance(blockIdx.x);
     int buf = 0;
     uint32_t par_bits = 0u;    // phase parity per barrier (bit k)
-    uint32_t pend_bits = 0u;   // copies in flight per barrier (thread 0's view, bit k)
+    uint32_t pend_bits = 0u;   // copies in flight per barrier (the issuer's view, bit k)
     bool issued_ok = true;
-    if (tid == 0 && tile < ntiles) {
+    if (issuer && tile < ntiles) {
         issued_ok = issue(tile, 0, 0) && issue(tile, 1, 0);
         pend_bits = issued_ok ? 5u : 0u;
     }
-    // On a failed wait the whole block leaves together; thread 0 first waits
+    // On a failed wait the whole block leaves together; the issuer first waits
     // (bounded) for the copies it still has in flight.
     auto bail = [&]() {
-        if (tid == 0) {
+        if (issuer) {
             atomicOr(a0.status, HOW_STATUS_TMA_TIMEOUT);
             for (int k = 0; k < 3; ++k)
                 if ((pend_bits >> k) & 1u) mbar_wait_bounded(&bars[k], (par_bits >> k) & 1u, kWaitLimit);
@@ -434,31 +439,40 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         pend_bits &= ~(1u << buf);
         {
             const long long next = advance(tile + gridDim.x);
-            if (tid == 0 && next < ntiles) {
+            if (issuer && next < ntiles) {
                 issued_ok = issue(next, 0, buf ^ 1) && issued_ok;
                 pend_bits |= 1u << (buf ^ 1);
             }
         }
-        // MODE 1: this tile's routing decisions (formed by the routing pass),
-        // fetched now by asynchronous 4-byte copies of the aligned words that
-        // hold them, so their latency hides behind P1
-        int dec_shift = -1;   // byte of the word, -1: no valid face
+        // MODE 1: the routing pass's decisions for this tile's faces and one
+        // more on each side of every line (faces -1 .. F), fetched now by
+        // asynchronous 4-byte copies of the aligned words that hold them, so
+        // their latency hides behind P1
+        constexpr int FE = F + 2;
+        int dec_shift = -1;   // byte of the word, -1: no face
         if constexpr (MODE == 1) {
-            if (tid < NLF) {
-                const int l = tid / F, f = tid % F;
+            static_assert(NL * FE <= NT, "one fetched decision per thread");
+            if (tid < NL * FE) {
+                const int l = tid / FE, f = tid % FE - 1;
                 const int iface = c0 + f;
-                if (line_ok(l) && iface <= n) {
+                if (line_ok(l) && iface >= 0 && iface <= n) {
                     const unsigned char* src = a.route_next + line_off(l) + (long long)(iface + 2) * sstride;
                     dec_shift = (int)(reinterpret_cast<uintptr_t>(src) & 3u);
-                    cp_async4(&sDec[tid], reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3)));
+                    cp_async4(&sDecW[tid], reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3)));
                 }
             }
             cp_async_commit();
         }
+        // this stage's dt / d: loaded now, used in P5
+        const double dtdl_tile = *a.dtdl;
         mark(0);
 
         // ------------------------------------------------------------ P1
-        for (int t = tid; t < NLC; t += blockDim.x) {
+        // two threads per cell: the first forms primitives and fluxes, the
+        // second the eigenvalues (both from the same primitive arithmetic)
+        for (int tt = tid; tt < 2 * NLC; tt += blockDim.x) {
+            const bool eig = tt >= NLC;
+            const int t = eig ? tt - NLC : tt;
             const int l = t / C, cc = t % C;
             const double DD = qraw(0, l, cc), Mx = qraw(1, l, cc), My = qraw(2, l, cc);
             const double Mz = qraw(3, l, cc), Bx = qraw(4, l, cc), By = qraw(5, l, cc);
@@ -477,41 +491,48 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 EE = pg / (gam - 1.0) + 0.5 * (rho * vv2 + BB2);
                 irho = 1.0 / rho;
             }
-            const double HH = (EE + pg) * irho;
-            sP[0 * NLC + t] = rho; sP[1 * NLC + t] = vx; sP[2 * NLC + t] = vy; sP[3 * NLC + t] = vz;
-            sP[4 * NLC + t] = Bx; sP[5 * NLC + t] = By; sP[6 * NLC + t] = Bz; sP[7 * NLC + t] = pg;
-            sP[8 * NLC + t] = HH;
-            // eigenst centre (src/ssprk.cpp:561-593), with DD, EE the floored values
-            const double pt = pg + 0.5 * BB2;
-            const double vdB = vx * Bx + vy * By + vz * Bz;
-            const double bbn2 = BB2 * irho;
-            const double bnx2 = Bx * Bx * irho;
-            const double cs2 = fmax(0.0, gam * fabs(pg * irho));
-            const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
-            const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
-            if constexpr (MODE == 2 || MODE == 3) {
-                // the routing features' cell values, once per cell
-                sCF[0 * NLC + t] = (float)rho;
-                sCF[1 * NLC + t] = (float)pg;
-                sCF[2 * NLC + t] = sqrtf((float)BB2);
-                sCF[3 * NLC + t] = sqrtf((float)vv2);
-                sCF[4 * NLC + t] = (float)lf;
+            if (!eig) {
+                const double HH = (EE + pg) * irho;
+                sP[0 * NLC + t] = rho; sP[1 * NLC + t] = vx; sP[2 * NLC + t] = vy; sP[3 * NLC + t] = vz;
+                sP[4 * NLC + t] = Bx; sP[5 * NLC + t] = By; sP[6 * NLC + t] = Bz; sP[7 * NLC + t] = pg;
+                sP[8 * NLC + t] = HH;
+                // eigenst centre fluxes (src/ssprk.cpp:561-593), with DD, EE the floored values
+                const double pt = pg + 0.5 * BB2;
+                const double vdB = vx * Bx + vy * By + vz * Bz;
+                double* U = sUst + t * 14;
+                double* Fc = sFc + t * 7;
+                Fc[0] = U[0] = rho * vx;                 // DD (floored) * vx
+                Fc[1] = U[1] = Mx * vx + pt - Bx * Bx;
+                Fc[2] = U[2] = My * vx - Bx * By;
+                Fc[3] = U[3] = Mz * vx - Bx * Bz;
+                Fc[4] = U[4] = By * vx - Bx * vy;
+                Fc[5] = U[5] = Bz * vx - Bx * vz;
+                Fc[6] = U[6] = (EE + pt) * vx - Bx * vdB;
+                U[7] = rho; U[8] = Mx; U[9] = My; U[10] = Mz; U[11] = By; U[12] = Bz; U[13] = EE;
+            } else {
+                // eigenvalues (src/ssprk.cpp:561-593)
+                const double bbn2 = BB2 * irho;
+                const double bnx2 = Bx * Bx * irho;
+                const double cs2 = fmax(0.0, gam * fabs(pg * irho));
+                const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
+                const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
+                if constexpr (MODE != 0) {
+                    // the routing features' cell values, once per cell (the
+                    // guard of MODE 1 needs density and pressure only)
+                    sCF[0 * NLC + t] = (float)rho;
+                    sCF[1 * NLC + t] = (float)pg;
+                    if constexpr (MODE != 1) {
+                        sCF[2 * NLC + t] = sqrtf((float)BB2);
+                        sCF[3 * NLC + t] = sqrtf((float)vv2);
+                        sCF[4 * NLC + t] = (float)lf;
+                    }
+                }
+                const double la = sqrt(fmax(0.0, bnx2));
+                const double ls = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 - root)));
+                sA[0 * NLC + t] = R(vx - lf); sA[1 * NLC + t] = R(vx - la); sA[2 * NLC + t] = R(vx - ls);
+                sA[3 * NLC + t] = R(vx);      sA[4 * NLC + t] = R(vx + ls); sA[5 * NLC + t] = R(vx + la);
+                sA[6 * NLC + t] = R(vx + lf);
             }
-            const double la = sqrt(fmax(0.0, bnx2));
-            const double ls = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 - root)));
-            sA[0 * NLC + t] = R(vx - lf); sA[1 * NLC + t] = R(vx - la); sA[2 * NLC + t] = R(vx - ls);
-            sA[3 * NLC + t] = R(vx);      sA[4 * NLC + t] = R(vx + ls); sA[5 * NLC + t] = R(vx + la);
-            sA[6 * NLC + t] = R(vx + lf);
-            double* U = sUst + t * 14;
-            double* Fc = sFc + t * 7;
-            Fc[0] = U[0] = rho * vx;                 // DD (floored) * vx
-            Fc[1] = U[1] = Mx * vx + pt - Bx * Bx;
-            Fc[2] = U[2] = My * vx - Bx * By;
-            Fc[3] = U[3] = Mz * vx - Bx * Bz;
-            Fc[4] = U[4] = By * vx - Bx * vy;
-            Fc[5] = U[5] = Bz * vx - Bx * vz;
-            Fc[6] = U[6] = (EE + pt) * vx - Bx * vdB;
-            U[7] = rho; U[8] = Mx; U[9] = My; U[10] = Mz; U[11] = By; U[12] = Bz; U[13] = EE;
         }
         __syncthreads();
         mark(1);
@@ -561,10 +582,21 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             if constexpr (MODE == 1) {
                 // decisions of the learned router, formed for the whole sweep by
                 // the routing pass (route_prepass.cu) before this launch
-                static_assert(NLF <= NT, "one decision per thread");
+                // a face takes full WENO when the pass flagged it or a neighbour
+                // along the sweep (decisions formed once per step stay valid
+                // while a feature moves by up to one cell)
                 cp_async_wait_all();
+                if (tid < NL * FE)
+                    sDecW[tid] = dec_shift < 0 ? 0 : (int)((((unsigned int)sDecW[tid]) >> (8 * dec_shift)) & 0xffu);
+                __syncthreads();
                 if (tid < NLF) {
-                    sDec[tid] = dec_shift < 0 ? 0 : (int)((((unsigned int)sDec[tid]) >> (8 * dec_shift)) & 0xffu);
+                    const int l = tid / F, f = tid % F;
+                    const int* d = sDecW + l * FE + f;   // faces f-1, f, f+1
+                    // the hard guard on this stage's state, whatever the stage
+                    // the network's decisions were formed at
+                    const bool guard = router_guard_rp(sCF + l * C + f, sCF + NLC + l * C + f, (float)a.rhomin,
+                                                       (float)a.pgmin, a.guard_jump, a.guard_floor);
+                    sDec[tid] = (guard || (d[0] | d[1] | d[2])) ? 1 : 0;
                     row_amx(tid);
                 }
                 __syncthreads();
@@ -961,7 +993,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         }
         par_bits ^= 4u;
         pend_bits &= ~4u;
-        const double dtdl = *a.dtdl;
+        const double dtdl = dtdl_tile;
         for (int t = tid; t < 8 * NL * T; t += blockDim.x) {
             int v, l, ct;
             if (DIR == 0) { v = t / (NL * T); const int r = t % (NL * T); l = r / T; ct = r % T; }
@@ -985,7 +1017,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         __syncthreads();   // every read of the update operand / raw tile is done
         {
             const long long next = advance(tile + gridDim.x);
-            if (tid == 0 && next < ntiles) {
+            if (issuer && next < ntiles) {
                 issued_ok = issue(next, 1, 0) && issued_ok;
                 pend_bits |= 4u;
             }

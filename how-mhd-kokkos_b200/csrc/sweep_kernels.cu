@@ -104,7 +104,18 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     a.ct4 = c.p.ct_avg == 4;
     const bool mixed = c.precision == HOW_PREC_MIXED;
     const int mode = c.route_mode;
-    if (mode == 1) launch_route(c, dir, a.qprev, a.route_prev, a.route_next);
+    if (mode == 1) {
+        // learned routing: the routing pass forms fresh decisions (every
+        // route_refresh stages, starting at a step's first) into the other half of this
+        // direction's pair, which then becomes the current one; the sweep
+        // reads the current decisions
+        if ((c.cur_stage - 1) % c.route_refresh == 0) {
+            launch_route(c, dir, a.qprev, a.route_prev, a.route_next);
+            c.route_par[dir] ^= 1;
+        }
+        a.route_next = c.route_prev + (size_t)(2 * dir + c.route_par[dir]) * c.g.fs;
+        a.route_prev = nullptr;
+    }
     // instantiations: {fp64, mixed} x {plain, learned, guard-only}; label
     // collection runs the FP64 method
 #define HOW_SWEEP_CASES(D)                                                                              \
@@ -124,7 +135,7 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     if (dir == 0) HOW_SWEEP_CASES(0);
     else if (dir == 1) HOW_SWEEP_CASES(1);
     else HOW_SWEEP_CASES(2);
-    if (mode != 0) c.route_par[dir] ^= 1;
+    if (mode == 2 || mode == 3) c.route_par[dir] ^= 1;
 #undef HOW_SWEEP_CASES
 }
 

@@ -125,6 +125,7 @@ def _load():
         "how_router_set_weights": ([V, F, ctypes.c_int], ctypes.c_int),
         "how_router_configure": ([V, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float], ctypes.c_int),
         "how_router_stats": ([V, U64P, U64P, ctypes.c_int], ctypes.c_int),
+        "how_router_set_refresh": ([V, ctypes.c_int], ctypes.c_int),
         "how_router_stats4": ([V, U64P, U64P, U64P, U64P, ctypes.c_int], ctypes.c_int),
         "how_collect_begin": ([V, ctypes.c_uint, ctypes.c_uint], ctypes.c_int),
         "how_collect_end": ([V, F, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)], ctypes.c_int),
@@ -362,6 +363,12 @@ class Domain:
             w = _f32(weights, ROUTER_PARAMS)
             _check(_lib.how_router_set_weights(self._h, _fptr(w), w.size))
         _check(_lib.how_router_configure(self._h, m, threshold, guard_jump, guard_floor))
+
+    def set_router_refresh(self, stages):
+        """Learned routing: the network's decisions every `stages` SSPRK
+        stages (5 = once per step, the default; 1 = every stage); the guard is
+        evaluated at every stage."""
+        _check(_lib.how_router_set_refresh(self._h, int(stages)))
 
     def router_stats(self, reset=False, groups=False):
         """(full, cheap) interface counts since the last reset; with groups=True
