@@ -314,10 +314,20 @@ int init_turb3d(double* qp, const how_params* p, void*) {
                 const size_t o = ((size_t)i * ny + j) * nz + k;
                 V[o] = v[0]; V[ncell + o] = v[1]; V[2 * ncell + o] = v[2];
             }
+    // mean square speed: per-plane partial sums in parallel, then added in a
+    // fixed order, so the state is bitwise reproducible for a seed whatever
+    // the thread count
+    std::vector<double> part(nx, 0.0);
+    const size_t plane = (size_t)ny * nz;
+#pragma omp parallel for
+    for (int i = 0; i < nx; ++i) {
+        double s = 0.0;
+        for (size_t o = (size_t)i * plane; o < (size_t)(i + 1) * plane; ++o)
+            s += V[o] * V[o] + V[ncell + o] * V[ncell + o] + V[2 * ncell + o] * V[2 * ncell + o];
+        part[i] = s;
+    }
     double sum2 = 0.0;
-#pragma omp parallel for reduction(+ : sum2)
-    for (long long o = 0; o < (long long)ncell; ++o)
-        sum2 += V[o] * V[o] + V[ncell + o] * V[ncell + o] + V[2 * ncell + o] * V[2 * ncell + o];
+    for (int i = 0; i < nx; ++i) sum2 += part[i];
     const double scale = sum2 > 0.0 ? vrms / std::sqrt(sum2 / (double)ncell) : 0.0;
 #pragma omp parallel for collapse(2)
     for (int i = 0; i < nx; ++i)
