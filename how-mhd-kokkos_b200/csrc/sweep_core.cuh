@@ -546,6 +546,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         }
         if constexpr (MODE != 0) {
             if (tid < 2) s_cnt[tid] = 0u;
+            if (tid == 0) s_nfull = 0;
         }
         __syncthreads();
         mark(2);
@@ -596,7 +597,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     // the network's decisions were formed at
                     const bool guard = router_guard_rp(sCF + l * C + f, sCF + NLC + l * C + f, (float)a.rhomin,
                                                        (float)a.pgmin, a.guard_jump, a.guard_floor);
-                    sDec[tid] = (guard || (d[0] | d[1] | d[2])) ? 1 : 0;
+                    const bool full = guard || (d[0] | d[1] | d[2]);
+                    sDec[tid] = full ? 1 : 0;
+                    // list of full-WENO interfaces: P2a-P4 treat each entry on
+                    // its own, so the order the atomic gives does not matter
+                    if (full) sList[atomicAdd(&s_nfull, 1)] = tid;
                     row_amx(tid);
                 }
                 __syncthreads();
@@ -615,29 +620,21 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                         sDev[t] = 0.0f;
                     }
                     sDec[t] = MODE == 3 ? 1 : (guard ? 1 : 0);
+                    if constexpr (MODE == 2) {
+                        if (guard) sList[atomicAdd(&s_nfull, 1)] = t;
+                    }
                 }
                 __syncthreads();
                 mark(3);
             }
-            if constexpr (ROUTED) {
-                if (tid < 32) {   // compaction by one warp
-                    int base = 0;
-                    for (int c0w = 0; c0w < NLF; c0w += 32) {
-                        const int t = c0w + tid;
-                        const bool full = t < NLF && sDec[t] != 0;
-                        const unsigned int m = __ballot_sync(0xffffffffu, full);
-                        if (full) sList[base + __popc(m & ((1u << tid) - 1u))] = t;
-                        base += __popc(m);
-                    }
-                    if (tid == 0) s_nfull = base;
-                }
-                __syncthreads();
-                nfull = s_nfull;
-            }
+            if constexpr (ROUTED) nfull = s_nfull;
         }
 
         mark(5);
 
+        // A routed tile with no full-WENO interface skips P2a-P3 and their
+        // barriers (nfull is the same for the whole block)
+        if (!ROUTED || nfull > 0) {
         // ------------------------------------------------------------ P2a
         for (int k = tid; k < nfull; k += blockDim.x) {
             const int t = ROUTED ? sList[k] : k;
@@ -897,6 +894,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             }
         }
         __syncthreads();
+        }   // P2a-P3
         mark(8);
 
         // ------------------------------------------------------------ P4
