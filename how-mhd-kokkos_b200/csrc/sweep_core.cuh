@@ -548,6 +548,12 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             if (tid < 2) s_cnt[tid] = 0u;
             if (tid == 0) s_nfull = 0;
         }
+        if constexpr (MODE == 1) {
+            // the fetched decision words have arrived: keep this thread's byte
+            cp_async_wait_all();
+            if (tid < NL * FE)
+                sDecW[tid] = dec_shift < 0 ? 0 : (int)((((unsigned int)sDecW[tid]) >> (8 * dec_shift)) & 0xffu);
+        }
         __syncthreads();
         mark(2);
 
@@ -586,10 +592,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 // a face takes full WENO when the pass flagged it or a neighbour
                 // along the sweep (decisions formed once per step stay valid
                 // while a feature moves by up to one cell)
-                cp_async_wait_all();
-                if (tid < NL * FE)
-                    sDecW[tid] = dec_shift < 0 ? 0 : (int)((((unsigned int)sDecW[tid]) >> (8 * dec_shift)) & 0xffu);
-                __syncthreads();
+                bool owned = false, full = false;
                 if (tid < NLF) {
                     const int l = tid / F, f = tid % F;
                     const int* d = sDecW + l * FE + f;   // faces f-1, f, f+1
@@ -597,12 +600,22 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     // the network's decisions were formed at
                     const bool guard = router_guard_rp(sCF + l * C + f, sCF + NLC + l * C + f, (float)a.rhomin,
                                                        (float)a.pgmin, a.guard_jump, a.guard_floor);
-                    const bool full = guard || (d[0] | d[1] | d[2]);
+                    full = guard || (d[0] | d[1] | d[2]);
                     sDec[tid] = full ? 1 : 0;
                     // list of full-WENO interfaces: P2a-P4 treat each entry on
                     // its own, so the order the atomic gives does not matter
                     if (full) sList[atomicAdd(&s_nfull, 1)] = tid;
                     row_amx(tid);
+                    // counted once per face: a tile's last face is the next
+                    // tile's first, owned by the lower tile unless it ends the line
+                    const int iface = c0 + f;
+                    owned = line_ok(l) && iface <= n && (f < T || iface == n);
+                }
+                const unsigned int mf = __ballot_sync(0xffffffffu, owned && full);
+                const unsigned int mc = __ballot_sync(0xffffffffu, owned && !full);
+                if ((tid & 31) == 0) {
+                    if (mf) atomicAdd(&s_cnt[0], (unsigned int)__popc(mf));
+                    if (mc) atomicAdd(&s_cnt[1], (unsigned int)__popc(mc));
                 }
                 __syncthreads();
                 mark(3);
@@ -951,8 +964,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 // lower tile owns it unless it is the line's last face
                 if (valid && r == 0 && (f < T || iface == n)) {
                     const long long o = line_off(l) + (long long)(iface + 2) * sstride;
-                    if constexpr (ROUTED) {
-                        if constexpr (MODE == 2) a.route_next[o] = (unsigned char)(full ? 1 : 0);
+                    if constexpr (MODE == 2) {
+                        a.route_next[o] = (unsigned char)(full ? 1 : 0);
                         atomicAdd(&s_cnt[full ? 0 : 1], 1u);
                     }
                     if constexpr (MODE == 3) {
