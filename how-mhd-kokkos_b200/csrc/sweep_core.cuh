@@ -510,12 +510,15 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 Fc[6] = U[6] = (EE + pt) * vx - Bx * vdB;
                 U[7] = rho; U[8] = Mx; U[9] = My; U[10] = Mz; U[11] = By; U[12] = Bz; U[13] = EE;
             } else {
-                // eigenvalues (src/ssprk.cpp:561-593)
-                const double bbn2 = BB2 * irho;
-                const double bnx2 = Bx * Bx * irho;
-                const double cs2 = fmax(0.0, gam * fabs(pg * irho));
-                const double root = sqrt(fmax(0.0, (bbn2 + cs2) * (bbn2 + cs2) - 4.0 * bnx2 * cs2));
-                const double lf = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 + root)));
+                // eigenvalues (src/ssprk.cpp:561-593), in the working type R:
+                // FP64 for the plain method, FP32 in the mixed one (where they
+                // feed only the FP32 characteristic part)
+                const R irR = R(irho);
+                const R bbn2 = R(BB2) * irR;
+                const R bnx2 = R(Bx * Bx) * irR;
+                const R cs2 = fmax(R(0), gamR * fabs(R(pg) * irR));
+                const R root = Math<R>::sq(fmax(R(0), (bbn2 + cs2) * (bbn2 + cs2) - R(4) * bnx2 * cs2));
+                const R lf = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 + root)));
                 if constexpr (MODE != 0) {
                     // the routing features' cell values, once per cell (the
                     // guard of MODE 1 needs density and pressure only)
@@ -527,11 +530,12 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                         sCF[4 * NLC + t] = (float)lf;
                     }
                 }
-                const double la = sqrt(fmax(0.0, bnx2));
-                const double ls = sqrt(fmax(0.0, 0.5 * (bbn2 + cs2 - root)));
-                sA[0 * NLC + t] = R(vx - lf); sA[1 * NLC + t] = R(vx - la); sA[2 * NLC + t] = R(vx - ls);
-                sA[3 * NLC + t] = R(vx);      sA[4 * NLC + t] = R(vx + ls); sA[5 * NLC + t] = R(vx + la);
-                sA[6 * NLC + t] = R(vx + lf);
+                const R la = Math<R>::sq(fmax(R(0), bnx2));
+                const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
+                const R vxR = R(vx);
+                sA[0 * NLC + t] = vxR - lf; sA[1 * NLC + t] = vxR - la; sA[2 * NLC + t] = vxR - ls;
+                sA[3 * NLC + t] = vxR;      sA[4 * NLC + t] = vxR + ls; sA[5 * NLC + t] = vxR + la;
+                sA[6 * NLC + t] = vxR + lf;
             }
         }
         __syncthreads();
