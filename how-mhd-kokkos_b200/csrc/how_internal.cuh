@@ -36,6 +36,18 @@ inline Grid make_grid(int nx, int ny, int nz) {
     return g;
 }
 
+// Per-face byte arrays of the learned router (decisions, priors), one per
+// sweep direction, laid out line-major so that a line's faces along the sweep
+// are contiguous in every direction: the face at padded index s of the line
+// through transverse padded indices (t1, t2) (x sweep: j, k; y sweep: i, k;
+// z sweep: i, j) is byte route_line(g, dir, t1, t2) + s.  A direction's
+// array holds at most P0 P1 P2 <= fs bytes.
+__host__ __device__ inline long long route_line(const Grid& g, int dir, int t1, int t2) {
+    if (dir == 0) return ((long long)t2 * g.P1 + t1) * g.P0;
+    if (dir == 1) return ((long long)t2 * g.P0 + t1) * g.P1;
+    return ((long long)t2 * g.P0 + t1) * g.P2;
+}
+
 // SSPRK(5,4) coefficients (src/ssprk.cpp:66-94)
 struct RKCoeff { double k1, k2, k3, k4, k5; };
 inline RKCoeff rk_coeff(int iw) {

@@ -153,7 +153,9 @@ __global__ void __launch_bounds__(kRouteThreads) k_route_x(const __grid_constant
     for (long long wi = (long long)blockIdx.x * (blockDim.x >> 5) + warp; wi < nwork; wi += wstride) {
         const int seg = (int)(wi % nseg);
         const long long ln = wi / nseg;
-        const long long line = g.idx(0, 3 + (int)(ln % g.ny), 3 + (int)(ln / g.ny));
+        const int lj = 3 + (int)(ln % g.ny), lk = 3 + (int)(ln / g.ny);
+        const long long line = g.idx(0, lj, lk);
+        const long long rl = route_line(g, 0, lj, lk);   // the line in the per-face arrays
         const int f0 = seg * 32;
         for (int k = lane; k < 37; k += 32) {
             const int s = f0 + k;   // padded cell index
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(kRouteThreads) k_route_x(const __grid_constant
         const bool live = iface <= n;
         float ft[kRouterNF] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         bool flat = true, guard = false;
-        const long long face = line + iface + 2;
+        const long long face = rl + iface + 2;
         if (live) {
             StencilCell sc[6];
 #pragma unroll
@@ -207,13 +209,14 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__
     for (long long base = (long long)blockIdx.x * blockDim.x; base < nwork; base += (long long)gridDim.x * blockDim.x) {
         const long long widx = base + tid;
         const bool valid = widx < nwork;
-        long long line = 0;
+        long long line = 0, rl = 0;
         int f0 = 0;
         if (valid) {
             const long long ln = widx % nlines;
             f0 = (int)(widx / nlines) * kSeg;
             const int ia = (int)(ln % la), ib = (int)(ln / la);
             line = DIR == 1 ? g.idx(3 + ia, 0, 3 + ib) : g.idx(3 + ia, 3 + ib, 0);
+            rl = route_line(g, DIR, 3 + ia, 3 + ib);   // the line in the per-face arrays
         }
         // window: stencil cells f .. f+5 of face f (padded cells)
         StencilCell win[6];
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__
             const bool live = valid && iface <= n;
             float ft[kRouterNF] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             bool flat = true, guard = false;
-            const long long face = line + (long long)(iface + 2) * stride;
+            const long long face = rl + iface + 2;
             if (live) {
                 win[5] = route_cell(a.q, g.fs, line + (long long)(iface + 5) * stride, DIR, a.gam, a.rhomin, a.pgmin);
                 guard = router_features(win, (float)a.prev[face], (float)a.rhomin, (float)a.pgmin, a.guard_jump,

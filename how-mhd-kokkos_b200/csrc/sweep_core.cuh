@@ -418,6 +418,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             return g.idx(t1, t2, 0);
         };
         auto line_ok = [&](int l) -> bool { return t1_0 + l >= 3 && t1_0 + l <= nt1 + 2; };
+        // the line's first byte in the router's per-face arrays (route_line)
+        auto rline = [&](int l) -> long long { return route_line(g, DIR, t1_0 + l, t2); };
         const double* sQ = reinterpret_cast<const double*>(sm + TL::bQ + buf * align_up(8 * TL::NQ, 128));
         const double* sO = reinterpret_cast<const double*>(sm + TL::bO);
         // raw conserved of line variable v at (line l, tile cell c); box order
@@ -456,7 +458,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 const int l = tid / FE, f = tid % FE - 1;
                 const int iface = c0 + f;
                 if (line_ok(l) && iface >= 0 && iface <= n) {
-                    const unsigned char* src = a.route_next + line_off(l) + (long long)(iface + 2) * sstride;
+                    const unsigned char* src = a.route_next + rline(l) + (iface + 2);
                     dec_shift = (int)(reinterpret_cast<uintptr_t>(src) & 3u);
                     cp_async4(&sDecW[tid], reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3)));
                 }
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 }
                 const int iface = c0 + f;
                 prior = 1.0f;
-                if (line_ok(l) && iface <= n) prior = (float)a.route_prev[line_off(l) + (long long)(iface + 2) * sstride];
+                if (line_ok(l) && iface <= n) prior = (float)a.route_prev[rline(l) + (iface + 2)];
                 return router_features(sc, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump, a.guard_floor, ft,
                                        &flat);
             };
@@ -967,7 +969,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 // a tile's last interface is also the next tile's first: the
                 // lower tile owns it unless it is the line's last face
                 if (valid && r == 0 && (f < T || iface == n)) {
-                    const long long o = line_off(l) + (long long)(iface + 2) * sstride;
+                    const long long o = rline(l) + (iface + 2);
                     if constexpr (MODE == 2) {
                         a.route_next[o] = (unsigned char)(full ? 1 : 0);
                         atomicAdd(&s_cnt[full ? 0 : 1], 1u);
