@@ -113,6 +113,15 @@ struct Tile {
     static constexpr int bCF = bAmx + align_up((int)sizeof(R) * NLF, 16);   // [5][NLC] float cell features
     static constexpr int bDecW = bCF + align_up(4 * 5 * NLC, 16);  // [NL][F+2] int: fetched decisions
     static constexpr int bEnd = bDecW + align_up(4 * NL * (F + 2), 16);
+    // learned routing (MODE 1) keeps only what it uses: decisions, list, LF
+    // speed, the cells' density and pressure (the guard), fetched decisions
+    static constexpr int lDec = bB + 32;
+    static constexpr int lList = lDec + align_up(4 * NLF, 16);
+    static constexpr int lAmx = lList + align_up(4 * NLF, 16);
+    static constexpr int lCF = lAmx + align_up((int)sizeof(R) * NLF, 16);
+    static constexpr int lDecW = lCF + align_up(4 * 2 * NLC, 16);
+    static constexpr int lEnd = lDecW + align_up(4 * NL * (F + 2), 16);
+    static constexpr size_t bytes_learned = (size_t)lEnd;
     static constexpr size_t bytes_plain = (size_t)bB + 3 * 8;
     static constexpr size_t bytes_route = (size_t)bEnd;
     static constexpr uint32_t in_bytes = 8u * NQ;
@@ -250,13 +259,14 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     R* sFs = sS;                                                       // [7][NI], after P2b
     double* sdF = reinterpret_cast<double*>(sm + TL::bS + TL::offdF);   // [7][NI], after P3
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TL::bB);
-    int* sDec = reinterpret_cast<int*>(sm + TL::bDec);          // 1: full WENO, 0: linear flux
-    int* sList = reinterpret_cast<int*>(sm + TL::bList);        // full-WENO interfaces, compacted
+    constexpr bool LM = MODE == 1;   // the learned mode's compact layout
+    int* sDec = reinterpret_cast<int*>(sm + (LM ? TL::lDec : TL::bDec));       // 1: full WENO, 0: linear flux
+    int* sList = reinterpret_cast<int*>(sm + (LM ? TL::lList : TL::bList));    // full-WENO interfaces
     float* sDev = reinterpret_cast<float*>(sm + TL::bDev);      // weight deviation (collect)
     float* sFt = reinterpret_cast<float*>(sm + TL::bFt);        // features (collect)
-    R* sAmx = reinterpret_cast<R*>(sm + TL::bAmx);              // per interface: max |lambda_0|, |lambda_6|
-    float* sCF = reinterpret_cast<float*>(sm + TL::bCF);        // per cell: rho, p, |B|, |v|, c_f (routing)
-    int* sDecW = reinterpret_cast<int*>(sm + TL::bDecW);        // MODE 1: fetched decisions (words, then bytes)
+    R* sAmx = reinterpret_cast<R*>(sm + (LM ? TL::lAmx : TL::bAmx));           // per interface: max |lambda_0|, |lambda_6|
+    float* sCF = reinterpret_cast<float*>(sm + (LM ? TL::lCF : TL::bCF));      // per cell: rho, p, |B|, |v|, c_f
+    int* sDecW = reinterpret_cast<int*>(sm + (LM ? TL::lDecW : TL::bDecW));    // MODE 1: fetched decisions
     __shared__ int s_nfull;
     __shared__ unsigned int s_cnt[2];   // full, cheap interfaces
 

@@ -11,7 +11,7 @@ namespace {
 template <int DIR, int NL, int T, int NT, typename R, int MINB, int MODE>
 void launch_one(Ctx& c, const SweepArgs& a) {
     using TL = Tile<DIR, NL, T, R>;
-    constexpr size_t bytes = (MODE == 0 ? TL::bytes_plain : TL::bytes_route) + 128;
+    constexpr size_t bytes = (MODE == 0 ? TL::bytes_plain : MODE == 1 ? TL::bytes_learned : TL::bytes_route) + 128;
     static bool attr_done = false;
     if (!attr_done) {
         cudaFuncSetAttribute(k_sweep<DIR, NL, T, NT, R, MINB, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -123,7 +123,7 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
         using S = SweepShape<D>;                                                                        \
         if (mode == 3) { launch_one<D, S::NL, S::T, 128, double, 3, 3>(c, a); break; }                  \
         if (mixed) {                                                                                    \
-            if (mode == 1) launch_one<D, S::NL, S::T, 128, float, 5, 1>(c, a);                          \
+            if (mode == 1) launch_one<D, S::NL, S::T, 128, float, 6, 1>(c, a);                          \
             else if (mode == 2) launch_one<D, S::NL, S::T, 128, float, 5, 2>(c, a);                     \
             else launch_one<D, S::NL, S::T, 128, float, 6, 0>(c, a);                                    \
         } else {                                                                                        \
