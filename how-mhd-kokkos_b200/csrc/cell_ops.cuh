@@ -25,15 +25,41 @@ __device__ __forceinline__ void op_bound_column(const Grid& g, double* field, in
     double* A = field + base;
     auto at = [&](int s) -> double& { return A[s * stride]; };
     if (periodic) {
-        at(0) = at(n); at(1) = at(n + 1); at(2) = at(n + 2);
-        at(n + 3) = at(3); at(n + 4) = at(4); at(n + 5) = at(5);
+        if (n >= 3) {
+            // no source index is a ghost: all six loads go out together
+            const double s0 = at(n), s1 = at(n + 1), s2 = at(n + 2), s3 = at(3), s4 = at(4), s5 = at(5);
+            at(0) = s0; at(1) = s1; at(2) = s2;
+            at(n + 3) = s3; at(n + 4) = s4; at(n + 5) = s5;
+        } else {
+            at(0) = at(n); at(1) = at(n + 1); at(2) = at(n + 2);
+            at(n + 3) = at(3); at(n + 4) = at(4); at(n + 5) = at(5);
+        }
     } else {
-        const double lo = at(3);
+        const double lo = at(3), hi = at(n + 2);
         at(0) = lo; at(1) = lo; at(2) = lo;
-        const double hi = at(n + 2);
         at(n + 3) = hi; at(n + 4) = hi; at(n + 5) = hi;
     }
 }
+// The padded index whose value the ghost fill above leaves at padded index s
+// of an axis with n >= 2 active cells: the identity on [3, n+2], and an
+// active index for every s in [1, n+4].
+__host__ __device__ __forceinline__ int bc_map(int s, int n, int periodic) {
+    if (s < 3) return periodic ? s + n : 3;
+    if (s > n + 2) return periodic ? s - n : n + 2;
+    return s;
+}
+
+// How the CT bodies below reach a neighbour of an active cell along an axis:
+// on = 0, at the plain offset (the array's ghosts were filled); on = 1,
+// through bc_map (they were not: the read returns what the fill would have
+// put there).  p*: the periodic axes.
+struct BCMap { int px, py, pz, on; };
+
+// (stride * 5 fits an int for every grid the device memory holds)
+__device__ __forceinline__ int nb_off(const BCMap& m, int s, int d, int n, int periodic, int stride) {
+    return m.on ? (bc_map(s + d, n, periodic) - s) * stride : d * stride;
+}
+
 // columns of one field: (fast transverse extent, slow transverse extent)
 template <int AX>
 __host__ __device__ __forceinline__ void bound_plane(const Grid& g, int& ta, int& tb) {
@@ -60,13 +86,16 @@ __device__ __forceinline__ void op_tstep_cell(const Grid& g, const double* __res
     const double Bx = q[4 * g.fs + c], By = q[5 * g.fs + c], Bz = q[6 * g.fs + c];
     const double EE = q[7 * g.fs + c];
     const double rho = fmax(DD, rhomin);
-    const double vx = Mx / rho, vy = My / rho, vz = Mz / rho;
+    // the seven quotients by rho, each correctly rounded, from one division
+    const double ir = 1.0 / rho;
+    const double vx = div_const(Mx, rho, ir), vy = div_const(My, rho, ir), vz = div_const(Mz, rho, ir);
     const double vv2 = vx * vx + vy * vy + vz * vz;
     const double BB2 = Bx * Bx + By * By + Bz * Bz;
     const double pg = fmax(pgmin, (gam - 1.0) * (EE - 0.5 * (rho * vv2 + BB2)));
-    const double bbn2 = BB2 / rho;
-    const double cs2 = fmax(0.0, gam * pg / rho);
-    const double bnx2 = Bx * Bx / rho, bny2 = By * By / rho, bnz2 = Bz * Bz / rho;
+    const double bbn2 = div_const(BB2, rho, ir);
+    const double cs2 = fmax(0.0, div_const(gam * pg, rho, ir));
+    const double bnx2 = div_const(Bx * Bx, rho, ir), bny2 = div_const(By * By, rho, ir),
+                 bnz2 = div_const(Bz * Bz, rho, ir);
     const double s = (bbn2 + cs2) * (bbn2 + cs2);
     const double rootx = sqrt(fmax(0.0, s - 4.0 * bnx2 * cs2));
     const double rooty = sqrt(fmax(0.0, s - 4.0 * bny2 * cs2));
@@ -145,12 +174,13 @@ __device__ __forceinline__ void op_prot_cell(const Grid& g, double* __restrict__
     const double Bx = q[4 * g.fs + c], By = q[5 * g.fs + c], Bz = q[6 * g.fs + c];
     double E = q[7 * g.fs + c];
     rho = fmax(rho, rhomin);
-    const double vx = Mx / rho, vy = My / rho, vz = Mz / rho;
+    const double irho = 1.0 / rho, igm1 = 1.0 / (gam - 1.0);
+    const double vx = div_const(Mx, rho, irho), vy = div_const(My, rho, irho), vz = div_const(Mz, rho, irho);
     const double vv2 = vx * vx + vy * vy + vz * vz;
     const double BB2 = Bx * Bx + By * By + Bz * Bz;
     double pg = (gam - 1.0) * (E - 0.5 * (rho * vv2 + BB2));
     pg = fmax(pg, pgmin);
-    E = pg / (gam - 1.0) + 0.5 * (rho * vv2 + BB2);
+    E = div_const(pg, gam - 1.0, igm1) + 0.5 * (rho * vv2 + BB2);
     q[c] = rho;
     q[7 * g.fs + c] = E;
 }
@@ -160,11 +190,14 @@ __device__ __forceinline__ void op_stage5_cell(const Grid& g, const double* __re
                                                const double* __restrict__ q2, const double* __restrict__ q3,
                                                double* __restrict__ q5, double c4, double c5, int i, int j, int k) {
     const long long c = g.idx(i, j, k);
+    double r[8];
 #pragma unroll
     for (int v = 0; v < 8; ++v) {
         const long long o = v * g.fs + c;
-        q5[o] = q0[o] + c4 * q2[o] + c5 * q3[o];
+        r[v] = q0[o] + c4 * q2[o] + c5 * q3[o];
     }
+#pragma unroll
+    for (int v = 0; v < 8; ++v) q5[v * g.fs + c] = r[v];
 }
 
 // ---------------------------------------------------------------- CT
@@ -177,20 +210,40 @@ __host__ __device__ __forceinline__ CTFields ct_fields(double* const* ct) {
     return CTFields{ct[0], ct[1], ct[2], ct[3], ct[4], ct[5], ct[6], ct[7], ct[8], ct[9], ct[10], ct[11]};
 }
 
+// fluxct_build_O2's 4-point face average (src/fluxct.cpp:809-821)
+__device__ __forceinline__ double ct_avg4(double a, double b, double c, double d) {
+    return (-a + 9.0 * b + 9.0 * c - d) / 16.0;
+}
+// fluxct_smooth_O's two 3-point corrections (src/fluxct.cpp:828-840)
+__device__ __forceinline__ double ct_smooth(double o, double l1, double r1, double l2, double r2) {
+    return o + div_const(l1 - 2.0 * o + r1, 24.0, 1.0 / 24.0) + div_const(l2 - 2.0 * o + r2, 24.0, 1.0 / 24.0);
+}
+
 // fluxct_build_O2 (src/fluxct.cpp:809-821)
-__device__ __forceinline__ void op_emf2_cell(const Grid& g, const CTFields& f, int use_Ox, int use_Oy, int use_Oz,
-                                             int i, int j, int k) {
+__device__ __forceinline__ void op_emf2_cell(const Grid& g, const CTFields& f, const BCMap& m, int use_Ox,
+                                             int use_Oy, int use_Oz, int i, int j, int k) {
     const long long c = g.idx(i, j, k);
     const long long sj = g.pitch, sk = (long long)g.pitch * g.P1;
+    const int xm1 = nb_off(m, i, -1, g.nx, m.px, 1), xp1 = nb_off(m, i, 1, g.nx, m.px, 1),
+              xp2 = nb_off(m, i, 2, g.nx, m.px, 1);
+    const int ym1 = nb_off(m, j, -1, g.ny, m.py, (int)sj), yp1 = nb_off(m, j, 1, g.ny, m.py, (int)sj),
+              yp2 = nb_off(m, j, 2, g.ny, m.py, (int)sj);
+    const int zm1 = nb_off(m, k, -1, g.nz, m.pz, (int)sk), zp1 = nb_off(m, k, 1, g.nz, m.pz, (int)sk),
+              zp2 = nb_off(m, k, 2, g.nz, m.pz, (int)sk);
+    // every load before the first store (the compiler cannot rule out aliasing)
+    double ox = 0.0, oy = 0.0, oz = 0.0;
     if (use_Ox)
-        f.Ox2[c] = (-f.gsx[c - 1] + 9.0 * f.gsx[c] + 9.0 * f.gsx[c + 1] - f.gsx[c + 2]) / 16.0
-                 - (-f.fsy[c - sj] + 9.0 * f.fsy[c] + 9.0 * f.fsy[c + sj] - f.fsy[c + 2 * sj]) / 16.0;
+        ox = ct_avg4(f.gsx[c + xm1], f.gsx[c], f.gsx[c + xp1], f.gsx[c + xp2])
+           - ct_avg4(f.fsy[c + ym1], f.fsy[c], f.fsy[c + yp1], f.fsy[c + yp2]);
     if (use_Oy)
-        f.Oy2[c] = (-f.hsy[c - sj] + 9.0 * f.hsy[c] + 9.0 * f.hsy[c + sj] - f.hsy[c + 2 * sj]) / 16.0
-                 - (-f.gsz[c - sk] + 9.0 * f.gsz[c] + 9.0 * f.gsz[c + sk] - f.gsz[c + 2 * sk]) / 16.0;
+        oy = ct_avg4(f.hsy[c + ym1], f.hsy[c], f.hsy[c + yp1], f.hsy[c + yp2])
+           - ct_avg4(f.gsz[c + zm1], f.gsz[c], f.gsz[c + zp1], f.gsz[c + zp2]);
     if (use_Oz)
-        f.Oz2[c] = (-f.fsz[c - sk] + 9.0 * f.fsz[c] + 9.0 * f.fsz[c + sk] - f.fsz[c + 2 * sk]) / 16.0
-                 - (-f.hsx[c - 1] + 9.0 * f.hsx[c] + 9.0 * f.hsx[c + 1] - f.hsx[c + 2]) / 16.0;
+        oz = ct_avg4(f.fsz[c + zm1], f.fsz[c], f.fsz[c + zp1], f.fsz[c + zp2])
+           - ct_avg4(f.hsx[c + xm1], f.hsx[c], f.hsx[c + xp1], f.hsx[c + xp2]);
+    if (use_Ox) f.Ox2[c] = ox;
+    if (use_Oy) f.Oy2[c] = oy;
+    if (use_Oz) f.Oz2[c] = oz;
 }
 
 // fluxct_smooth_O (src/fluxct.cpp:828-840)
@@ -198,21 +251,13 @@ __device__ __forceinline__ void op_emf_cell(const Grid& g, const CTFields& f, in
                                             int i, int j, int k) {
     const long long c = g.idx(i, j, k);
     const long long sj = g.pitch, sk = (long long)g.pitch * g.P1;
-    if (use_Ox) {
-        const double o = f.Ox2[c];
-        f.Ox[c] = o + (f.Ox2[c - 1] - 2.0 * o + f.Ox2[c + 1]) / 24.0
-                    + (f.Ox2[c - sj] - 2.0 * o + f.Ox2[c + sj]) / 24.0;
-    }
-    if (use_Oy) {
-        const double o = f.Oy2[c];
-        f.Oy[c] = o + (f.Oy2[c - sj] - 2.0 * o + f.Oy2[c + sj]) / 24.0
-                    + (f.Oy2[c - sk] - 2.0 * o + f.Oy2[c + sk]) / 24.0;
-    }
-    if (use_Oz) {
-        const double o = f.Oz2[c];
-        f.Oz[c] = o + (f.Oz2[c - 1] - 2.0 * o + f.Oz2[c + 1]) / 24.0
-                    + (f.Oz2[c - sk] - 2.0 * o + f.Oz2[c + sk]) / 24.0;
-    }
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+    if (use_Ox) ox = ct_smooth(f.Ox2[c], f.Ox2[c - 1], f.Ox2[c + 1], f.Ox2[c - sj], f.Ox2[c + sj]);
+    if (use_Oy) oy = ct_smooth(f.Oy2[c], f.Oy2[c - sj], f.Oy2[c + sj], f.Oy2[c - sk], f.Oy2[c + sk]);
+    if (use_Oz) oz = ct_smooth(f.Oz2[c], f.Oz2[c - 1], f.Oz2[c + 1], f.Oz2[c - sk], f.Oz2[c + sk]);
+    if (use_Ox) f.Ox[c] = ox;
+    if (use_Oy) f.Oy[c] = oy;
+    if (use_Oz) f.Oz[c] = oz;
 }
 
 struct BArgs {
@@ -232,23 +277,32 @@ __device__ __forceinline__ double bbase(const BArgs& a, long long off) {
 
 // fluxct_update_bfield (src/fluxct.cpp:848-877) of one active cell.
 // Components the update does not touch keep the stage's copied/combined base.
-__device__ __forceinline__ void op_update_b_cell(const Grid& g, const CTFields& f, const BArgs& a, int use_Ox,
-                                                 int use_Oy, int use_Oz, int i, int j, int k) {
+__device__ __forceinline__ void op_update_b_cell(const Grid& g, const CTFields& f, const BArgs& a, const BCMap& m,
+                                                 int use_Ox, int use_Oy, int use_Oz, int i, int j, int k) {
     const long long c = g.idx(i, j, k);
     const long long sj = g.pitch, sk = (long long)g.pitch * g.P1;
+    const int xm2 = nb_off(m, i, -2, g.nx, m.px, 1), xm1 = nb_off(m, i, -1, g.nx, m.px, 1),
+              xp1 = nb_off(m, i, 1, g.nx, m.px, 1);
+    const int ym2 = nb_off(m, j, -2, g.ny, m.py, (int)sj), ym1 = nb_off(m, j, -1, g.ny, m.py, (int)sj),
+              yp1 = nb_off(m, j, 1, g.ny, m.py, (int)sj);
+    const int zm2 = nb_off(m, k, -2, g.nz, m.pz, (int)sk), zm1 = nb_off(m, k, -1, g.nz, m.pz, (int)sk),
+              zp1 = nb_off(m, k, 1, g.nz, m.pz, (int)sk);
     const double aa = 9.0 / 8.0, bb = -1.0 / 24.0;
     const double dtdx = a.dtdl[0], dtdy = a.dtdl[1], dtdz = a.dtdl[2];
     const long long fs = g.fs;
+    // the three components are formed before any is stored (the compiler
+    // cannot rule out aliasing, so a store would hold back later loads)
+    double r[3];
     {
         const long long o = c;
         const double base = bbase(a, o);
         if (use_Ox || use_Oz) {
             double dOx = 0.0, dOz = 0.0;
-            if (use_Ox) dOx = aa * (f.Ox[c] - f.Ox[c - sj]) + bb * (f.Ox[c + sj] - f.Ox[c - 2 * sj]);
-            if (use_Oz) dOz = aa * (f.Oz[c] - f.Oz[c - sk]) + bb * (f.Oz[c + sk] - f.Oz[c - 2 * sk]);
-            a.bout[o] = a.k1 * base + a.k3 * a.bprev[o] - dtdy * dOx + dtdz * dOz;
+            if (use_Ox) dOx = aa * (f.Ox[c] - f.Ox[c + ym1]) + bb * (f.Ox[c + yp1] - f.Ox[c + ym2]);
+            if (use_Oz) dOz = aa * (f.Oz[c] - f.Oz[c + zm1]) + bb * (f.Oz[c + zp1] - f.Oz[c + zm2]);
+            r[0] = a.k1 * base + a.k3 * a.bprev[o] - dtdy * dOx + dtdz * dOz;
         } else {
-            a.bout[o] = base;
+            r[0] = base;
         }
     }
     {
@@ -256,11 +310,11 @@ __device__ __forceinline__ void op_update_b_cell(const Grid& g, const CTFields& 
         const double base = bbase(a, o);
         if (use_Oy || use_Ox) {
             double dOy = 0.0, dOx = 0.0;
-            if (use_Oy) dOy = aa * (f.Oy[c] - f.Oy[c - sk]) + bb * (f.Oy[c + sk] - f.Oy[c - 2 * sk]);
-            if (use_Ox) dOx = aa * (f.Ox[c] - f.Ox[c - 1]) + bb * (f.Ox[c + 1] - f.Ox[c - 2]);
-            a.bout[o] = a.k1 * base + a.k3 * a.bprev[o] - dtdz * dOy + dtdx * dOx;
+            if (use_Oy) dOy = aa * (f.Oy[c] - f.Oy[c + zm1]) + bb * (f.Oy[c + zp1] - f.Oy[c + zm2]);
+            if (use_Ox) dOx = aa * (f.Ox[c] - f.Ox[c + xm1]) + bb * (f.Ox[c + xp1] - f.Ox[c + xm2]);
+            r[1] = a.k1 * base + a.k3 * a.bprev[o] - dtdz * dOy + dtdx * dOx;
         } else {
-            a.bout[o] = base;
+            r[1] = base;
         }
     }
     {
@@ -268,13 +322,16 @@ __device__ __forceinline__ void op_update_b_cell(const Grid& g, const CTFields& 
         const double base = bbase(a, o);
         if (use_Oz || use_Oy) {
             double dOz = 0.0, dOy = 0.0;
-            if (use_Oz) dOz = aa * (f.Oz[c] - f.Oz[c - 1]) + bb * (f.Oz[c + 1] - f.Oz[c - 2]);
-            if (use_Oy) dOy = aa * (f.Oy[c] - f.Oy[c - sj]) + bb * (f.Oy[c + sj] - f.Oy[c - 2 * sj]);
-            a.bout[o] = a.k1 * base + a.k3 * a.bprev[o] - dtdx * dOz + dtdy * dOy;
+            if (use_Oz) dOz = aa * (f.Oz[c] - f.Oz[c + xm1]) + bb * (f.Oz[c + xp1] - f.Oz[c + xm2]);
+            if (use_Oy) dOy = aa * (f.Oy[c] - f.Oy[c + ym1]) + bb * (f.Oy[c + yp1] - f.Oy[c + ym2]);
+            r[2] = a.k1 * base + a.k3 * a.bprev[o] - dtdx * dOz + dtdy * dOy;
         } else {
-            a.bout[o] = base;
+            r[2] = base;
         }
     }
+    a.bout[c] = r[0];
+    a.bout[fs + c] = r[1];
+    a.bout[2 * fs + c] = r[2];
 }
 
 // B(iw) = base (1-D runs, where fluxct returns early, src/fluxct.cpp:793)
@@ -299,19 +356,21 @@ __device__ __forceinline__ void op_interp_prot_cell(const Grid& g, const double*
                                - 25.0 * by[c + sj] + 3.0 * by[c + 2 * sj]) / 256.0 : by[c];
     const double Bz = use_z ? (3.0 * bz[c - 3 * sk] - 25.0 * bz[c - 2 * sk] + 150.0 * bz[c - sk] + 150.0 * bz[c]
                                - 25.0 * bz[c + sk] + 3.0 * bz[c + 2 * sk]) / 256.0 : bz[c];
-    q[4 * fs + c] = Bx;
-    q[5 * fs + c] = By;
-    q[6 * fs + c] = Bz;
     double rho = q[c];
     const double Mx = q[fs + c], My = q[2 * fs + c], Mz = q[3 * fs + c];
     double E = q[7 * fs + c];
+    q[4 * fs + c] = Bx;
+    q[5 * fs + c] = By;
+    q[6 * fs + c] = Bz;
     rho = fmax(rho, rhomin);
-    const double vx = Mx / rho, vy = My / rho, vz = Mz / rho;
+    // the four quotients of prot, each correctly rounded, from two divisions
+    const double irho = 1.0 / rho, igm1 = 1.0 / (gam - 1.0);
+    const double vx = div_const(Mx, rho, irho), vy = div_const(My, rho, irho), vz = div_const(Mz, rho, irho);
     const double vv2 = vx * vx + vy * vy + vz * vz;
     const double BB2 = Bx * Bx + By * By + Bz * Bz;
     double pg = (gam - 1.0) * (E - 0.5 * (rho * vv2 + BB2));
     pg = fmax(pg, pgmin);
-    E = pg / (gam - 1.0) + 0.5 * (rho * vv2 + BB2);
+    E = div_const(pg, gam - 1.0, igm1) + 0.5 * (rho * vv2 + BB2);
     q[c] = rho;
     q[7 * fs + c] = E;
 }

@@ -3,8 +3,10 @@
 // The reference builds O2 over [0,n+3], smooths over [1,n+4] and updates face
 // B over [1,n+3], each followed by a full ghost fill that overwrites every
 // index outside [3, n+2] (src/fluxct.cpp:826, 846, 880).  Only active-index
-// results survive those fills, so these kernels compute active cells only and
-// then run the same ghost fill.  Face B: bxb(i) is the x-face at i+1/2.
+// results survive those fills, so these kernels compute active cells only.
+// O2, O and face B are then ghost-filled as there; the flux arrays are not,
+// and their reader goes through bc_map, which returns what the fill would
+// have left at a ghost index.  Face B: bxb(i) is the x-face at i+1/2.
 #include "cell_ops.cuh"
 
 namespace how {
@@ -16,9 +18,19 @@ namespace {
     const int j = 3 + blockIdx.y, k = 3 + blockIdx.z;                  \
     if (i > g.nx + 2) return
 
-__global__ void k_emf2(Grid g, CTFields f, int use_Ox, int use_Oy, int use_Oz) {
+// The flux arrays are never ghost-filled here: k_emf2 reads them through
+// bc_map (BCMap::on = 1), except in cells whose neighbours two out along
+// every stencilled axis are active, where the map is the identity and the
+// plain offsets serve.
+__device__ __forceinline__ bool ct_inner(const Grid& g, int i, int j, int k) {
+    return (g.nx == 1 || (i >= 5 && i <= g.nx)) && (g.ny == 1 || (j >= 5 && j <= g.ny)) &&
+           (g.nz == 1 || (k >= 5 && k <= g.nz));
+}
+
+__global__ void k_emf2(Grid g, CTFields f, BCMap m, int use_Ox, int use_Oy, int use_Oz) {
     HOW_CELL_IJK;
-    op_emf2_cell(g, f, use_Ox, use_Oy, use_Oz, i, j, k);
+    if (ct_inner(g, i, j, k)) op_emf2_cell(g, f, BCMap{0, 0, 0, 0}, use_Ox, use_Oy, use_Oz, i, j, k);
+    else op_emf2_cell(g, f, m, use_Ox, use_Oy, use_Oz, i, j, k);
 }
 
 __global__ void k_emf(Grid g, CTFields f, int use_Ox, int use_Oy, int use_Oz) {
@@ -28,7 +40,7 @@ __global__ void k_emf(Grid g, CTFields f, int use_Ox, int use_Oy, int use_Oz) {
 
 __global__ void k_update_b(Grid g, CTFields f, BArgs a, int use_Ox, int use_Oy, int use_Oz) {
     HOW_CELL_IJK;
-    op_update_b_cell(g, f, a, use_Ox, use_Oy, use_Oz, i, j, k);
+    op_update_b_cell(g, f, a, BCMap{0, 0, 0, 0}, use_Ox, use_Oy, use_Oz, i, j, k);
 }
 
 __global__ void k_faceb_base(Grid g, BArgs a) {
@@ -72,19 +84,14 @@ void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int s
     const int use_x = g.nx > 1, use_y = g.ny > 1, use_z = g.nz > 1;
     const int use_Ox = use_x && use_y, use_Oy = use_y && use_z, use_Oz = use_x && use_z;
     const CTFields f = ct_fields(c.ct);
-    // bound_ct_fluxes (src/fluxct.cpp:765-772) for the arrays the EMFs read
-    {
-        double* fl[6];
-        int n = 0;
-        if (use_Ox) { fl[n++] = c.ct[2]; fl[n++] = c.ct[0]; }           // gsx, fsy
-        if (use_Oy) { fl[n++] = c.ct[5]; fl[n++] = c.ct[3]; }           // hsy, gsz
-        if (use_Oz) { fl[n++] = c.ct[1]; fl[n++] = c.ct[4]; }           // fsz, hsx
-        launch_bound(c, fl, n);
-    }
-    dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
-    k_emf2<<<grid, 128, 0, c.stream>>>(g, f, use_Ox, use_Oy, use_Oz);
+    // bound_ct_fluxes (src/fluxct.cpp:765-772) is read through bc_map
+    // instead of run
+    const BCMap m{c.p.bc[0] == HOW_BC_PERIODIC, c.p.bc[1] == HOW_BC_PERIODIC, c.p.bc[2] == HOW_BC_PERIODIC, 1};
+    const dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
+    k_emf2<<<grid, 128, 0, c.stream>>>(g, f, m, use_Ox, use_Oy, use_Oz);
     ++c.launches;
     {
+        // the O2 ghost fill (src/fluxct.cpp:826)
         double* fl[3];
         int n = 0;
         if (use_Ox) fl[n++] = c.ct[6];
@@ -95,6 +102,9 @@ void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int s
     k_emf<<<grid, 128, 0, c.stream>>>(g, f, use_Ox, use_Oy, use_Oz);
     ++c.launches;
     {
+        // O is ghost-filled for the face-B update: its four-point differences
+        // reach two cells out, and a plain ghost fill costs less than mapping
+        // each of its nine neighbour offsets
         double* fl[3];
         int n = 0;
         if (use_Ox) fl[n++] = c.ct[9];

@@ -36,6 +36,23 @@ inline Grid make_grid(int nx, int ny, int nz) {
     return g;
 }
 
+// x / d, correctly rounded, for d > 0 given y = RN(1/d) (a compile-time
+// constant, or one IEEE division shared by several quotients): one multiply
+// and two FMAs in place of the division subroutine.  This is the correction
+// step of Markstein's division (IBM RS/6000, 1990): q0 = RN(x y) is within an
+// ulp of x/d, the remainder x - q0 d is exact in one FMA, and RN(q0 + rem y)
+// = RN(x/d).  A zero is returned as it is (x/d keeps its sign); when x or q0
+// is outside [2^-900, 2^900], where the remainder could leave the normal
+// range, or not finite, the plain division runs.
+__device__ __forceinline__ double div_const(double x, double d, double y) {
+    const double q0 = __dmul_rn(x, y);
+    const double q = __fma_rn(__fma_rn(-q0, d, x), y, q0);
+    const double ax = fabs(x), aq = fabs(q0);
+    if (ax >= 0x1p-900 && ax <= 0x1p+900 && aq >= 0x1p-900 && aq <= 0x1p+900) return q;
+    if (x == 0.0) return x;
+    return x / d;
+}
+
 // Per-face byte arrays of the learned router (decisions, priors), one per
 // sweep direction, laid out line-major so that a line's faces along the sweep
 // are contiguous in every direction: the face at padded index s of the line

@@ -971,7 +971,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     avg = (-x0 + 9.0 * x1 + 9.0 * x2 - x3) / 16.0;
                 } else {
                     // the reference's two-point form (-0, 9, 9, -0) / 18
-                    avg = (9.0 * x1 + 9.0 * x2) / 18.0;
+                    avg = div_const(9.0 * x1 + 9.0 * x2, 18.0, 1.0 / 18.0);
                 }
                 (r == 4 ? a.cta : a.ctb)[o] = dF + avg;
             }
