@@ -66,6 +66,8 @@ def parse():
                     help="ensemble: 64 uneven 2-D/1-D runs batched vs advanced one by one; "
                          "accuracy: whole blast run to --tend in every precision / routing form")
     ap.add_argument("--tend", type=float, default=0.2, help="end time of --workload accuracy")
+    ap.add_argument("--forms", default="",
+                    help="--workload accuracy: ';'-separated subset of the forms after fp64 (default: all)")
     return ap.parse_args()
 
 
@@ -576,6 +578,9 @@ def bench_accuracy(args):
     forms = [("fp64", "fp64", None, 5), ("mixed", "mixed", None, 5), ("mixed+learned", "mixed", "learned", 5),
              ("mixed+learned, decisions every stage", "mixed", "learned", 1),
              ("mixed+guard", "mixed", "guard", 5)]
+    if args.forms:
+        keep = {f.strip() for f in args.forms.split(";")}
+        forms = [f for f in forms if f[0] == "fp64" or f[0] in keep]   # FP64 is the reference
     out, ref = {}, None
     for name, prec, mode, refresh in forms:
         p = hm.read_parameters(workload_text(n, prec, tend=args.tend))
