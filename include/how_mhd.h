@@ -139,7 +139,9 @@ int how_prot(how_ctx* ctx, int stage);
  * stage 1 of ssprk with this dt: copies q(0) to q(1) first.  dir 0,1,2. */
 int how_sweep(how_ctx* ctx, int dir, double dt);
 /* Download a CT flux array (0..5 = fsy fsz gsx gsz hsx hsy) in the reference
- * layout, for inspection after how_sweep / how_ssprk. */
+ * layout, for inspection after how_sweep / how_ssprk.  Faces the sweeps
+ * compute are valid; ghost entries are not filled (the EMF kernel reads
+ * across the boundary through the ghost-fill index map instead). */
 int how_get_ct_array(how_ctx* ctx, int which, double* host);
 
 /* Main loop (src/main.cpp:158-223) without output: advances from *time for
