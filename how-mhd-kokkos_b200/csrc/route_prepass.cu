@@ -140,7 +140,8 @@ __device__ __forceinline__ void route_finish(RouteShared& S, const RouteArgs& a)
 // x sweeps: a warp takes 32 consecutive faces of one line; its lanes form
 // the values of 37 consecutive cells (coalesced along x) into shared memory
 // and each lane reads its face's 6.
-__global__ void __launch_bounds__(kRouteThreads) k_route_x(const __grid_constant__ RouteArgs a) {
+// (four blocks per SM: 63 registers without spills; the y/z kernels would spill)
+__global__ void __launch_bounds__(kRouteThreads, 4) k_route_x(const __grid_constant__ RouteArgs a) {
     __shared__ RouteShared S;
     __shared__ float cv[kRouteThreads / 32][37][5];
     route_setup(S, a);
