@@ -277,16 +277,13 @@ __device__ __forceinline__ double bbase(const BArgs& a, long long off) {
 
 // fluxct_update_bfield (src/fluxct.cpp:848-877) of one active cell.
 // Components the update does not touch keep the stage's copied/combined base.
-__device__ __forceinline__ void op_update_b_cell(const Grid& g, const CTFields& f, const BArgs& a, const BCMap& m,
-                                                 int use_Ox, int use_Oy, int use_Oz, int i, int j, int k) {
+__device__ __forceinline__ void op_update_b_cell(const Grid& g, const CTFields& f, const BArgs& a, int use_Ox,
+                                                 int use_Oy, int use_Oz, int i, int j, int k) {
     const long long c = g.idx(i, j, k);
     const long long sj = g.pitch, sk = (long long)g.pitch * g.P1;
-    const int xm2 = nb_off(m, i, -2, g.nx, m.px, 1), xm1 = nb_off(m, i, -1, g.nx, m.px, 1),
-              xp1 = nb_off(m, i, 1, g.nx, m.px, 1);
-    const int ym2 = nb_off(m, j, -2, g.ny, m.py, (int)sj), ym1 = nb_off(m, j, -1, g.ny, m.py, (int)sj),
-              yp1 = nb_off(m, j, 1, g.ny, m.py, (int)sj);
-    const int zm2 = nb_off(m, k, -2, g.nz, m.pz, (int)sk), zm1 = nb_off(m, k, -1, g.nz, m.pz, (int)sk),
-              zp1 = nb_off(m, k, 1, g.nz, m.pz, (int)sk);
+    const long long xm2 = -2, xm1 = -1, xp1 = 1;
+    const long long ym2 = -2 * sj, ym1 = -sj, yp1 = sj;
+    const long long zm2 = -2 * sk, zm1 = -sk, zp1 = sk;
     const double aa = 9.0 / 8.0, bb = -1.0 / 24.0;
     const double dtdx = a.dtdl[0], dtdy = a.dtdl[1], dtdz = a.dtdl[2];
     const long long fs = g.fs;

@@ -40,7 +40,7 @@ __global__ void k_emf(Grid g, CTFields f, int use_Ox, int use_Oy, int use_Oz) {
 
 __global__ void k_update_b(Grid g, CTFields f, BArgs a, int use_Ox, int use_Oy, int use_Oz) {
     HOW_CELL_IJK;
-    op_update_b_cell(g, f, a, BCMap{0, 0, 0, 0}, use_Ox, use_Oy, use_Oz, i, j, k);
+    op_update_b_cell(g, f, a, use_Ox, use_Oy, use_Oz, i, j, k);
 }
 
 __global__ void k_faceb_base(Grid g, BArgs a) {

@@ -154,7 +154,7 @@ __global__ void k_ens_cell(EnsDev d, const long long* __restrict__ start, int iw
         a.dtdl = &M.dsc->dtdl[iw][0];
         if constexpr (OP == OP_UPDATE_B) {
             const CTFields f = ct_fields(const_cast<double* const*>(M.ct));
-            op_update_b_cell(g, f, a, BCMap{0, 0, 0, 0}, M.use_Ox, M.use_Oy, M.use_Oz, i, j, k);
+            op_update_b_cell(g, f, a, M.use_Ox, M.use_Oy, M.use_Oz, i, j, k);
         } else {
             op_faceb_base_cell(g, a, i, j, k);
         }
