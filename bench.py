@@ -62,9 +62,11 @@ def parse():
     ap.add_argument("--t-start", type=float, default=0.05,
                     help="simulated time the timed steps start from (the blast evolved there first)")
     ap.add_argument("--no-fast", action="store_true", help="skip the mixed-precision + learned-routing leg")
-    ap.add_argument("--workload", default="blast", choices=["blast", "ensemble", "accuracy"],
+    ap.add_argument("--workload", default="blast", choices=["blast", "ensemble", "accuracy", "output"],
                     help="ensemble: 64 uneven 2-D/1-D runs batched vs advanced one by one; "
-                         "accuracy: whole blast run to --tend in every precision / routing form")
+                         "accuracy: whole blast run to --tend in every precision / routing form; "
+                         "output: dump files (how_output) of the blast state, .vts and .dat")
+    ap.add_argument("--out-dir", default="/tmp/how_dumps", help="--workload output: where the dumps go")
     ap.add_argument("--tend", type=float, default=0.2, help="end time of --workload accuracy")
     ap.add_argument("--forms", default="",
                     help="--workload accuracy: ';'-separated subset of the forms after fp64 (default: all)")
@@ -617,6 +619,41 @@ def bench_accuracy(args):
     return 0
 
 
+# --------------------------------------------------------------- output arm
+def bench_output(args):
+    """Dump files of the blast state at --n: how_output in both formats,
+    host clock around each synchronous call (device slab kernels, copies and
+    file writes), the best of three, with the file size and write rate.  The
+    reference writes the same files from host memory (src/output.cpp)."""
+    import os
+    import torch
+    import how_mhd as hm
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return 0
+    n = args.n
+    out = {}
+    for fmt in ("vts", "dat"):
+        p = hm.read_parameters(workload_text(n, "fp64") + f"output_format {fmt}\n")
+        with hm.Domain(p) as d:
+            d.init_problem()
+            d.run(0.0, 2)
+            d.sync()
+            best = None
+            for _ in range(3):
+                t0 = time.perf_counter()
+                path = d.output(2, 0.0, args.out_dir)
+                el = time.perf_counter() - t0
+                best = el if best is None else min(best, el)
+            size = os.path.getsize(path)
+            os.remove(path)
+        out[fmt] = {"s_per_dump": best, "bytes": size, "gb_per_s": size / best / 1e9}
+    print(json.dumps({"workload": f"dump files of blast3d_b {n}^3 (how_output)", "timing": "host clock, best of 3",
+                      "out_dir": args.out_dir, "formats": out}), flush=True)
+    return 0
+
+
 def ctypes_peak(hm):
     import ctypes
     v = ctypes.c_double()
@@ -632,6 +669,8 @@ def main():
         return bench_ensemble(args)
     if args.workload == "accuracy":
         return bench_accuracy(args)
+    if args.workload == "output":
+        return bench_output(args)
     return bench_ours(args)
 
 

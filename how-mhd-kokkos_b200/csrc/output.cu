@@ -1,0 +1,388 @@
+// output.cu -- dump files in the reference's formats (src/output.cpp): the
+// ASCII `.dat` table (output_dat, src/output.cpp:65-224) and the binary
+// appended-raw VTK StructuredGrid `.vts` (output_vts_binary,
+// src/output.cpp:226-552), chosen by output_format like output()
+// (src/output.cpp:555-572).
+//
+// The per-cell work -- velocities, gas pressure, v^2, B^2, the cell-centred
+// divB diagnostic, cell-centre coordinates, and the reordering into the
+// file's arrays -- runs on the GPU from q(0) in HBM, one slab of z planes at a
+// time, into the context's staging buffer.  Each slab is copied to the host
+// and written: the .vts blocks at their final file offsets (pwrite), the .dat
+// lines formatted by host threads.  Only the file assembly is host code.
+//
+// The values are the reference's bit for bit: every operation is a separately
+// rounded IEEE operation in the reference's evaluation order (the _rn
+// intrinsics, which the compiler never fuses into FMAs), and the text uses
+// the reference's stream format (std::scientific, precision 15 = "%.15e").
+#include "how_internal.cuh"
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace how {
+
+namespace {
+
+// bc_index_host (src/output.cpp:44-59): wrap over [lo, hi] when periodic,
+// else clamp.
+__device__ __forceinline__ int out_bc_index(int idx, int lo, int hi, int periodic) {
+    if (periodic) {
+        const int n = hi - lo + 1;
+        int r = (idx - lo) % n;
+        if (r < 0) r += n;
+        return lo + r;
+    }
+    return idx < lo ? lo : (idx > hi ? hi : idx);
+}
+
+struct DumpArgs {
+    Grid g;
+    const double* q;          // q(0), device layout
+    double* out;              // slab payload (staging buffer)
+    int k0, nk;               // slab: padded planes k0 .. k0 + nk - 1
+    int px, py, pz;           // periodic axes
+    double dx, dy, dz, gam;
+};
+
+// The quantities of one active cell (src/output.cpp:110-187 and 284-354).
+struct DumpCell {
+    double x, y, z, rho, Mx, My, Mz, Bx, By, Bz, E, pg, vx, vy, vz, vv2, BB2, divB;
+};
+
+__device__ __forceinline__ DumpCell dump_cell(const DumpArgs& a, int i, int j, int k) {
+    const Grid& g = a.g;
+    const long long fs = g.fs, c = g.idx(i, j, k);
+    DumpCell d;
+    d.x = __dmul_rn(__dadd_rn((double)(i - 3), 0.5), a.dx);
+    d.y = __dmul_rn(__dadd_rn((double)(j - 3), 0.5), a.dy);
+    d.z = __dmul_rn(__dadd_rn((double)(k - 3), 0.5), a.dz);
+    d.rho = a.q[c];
+    d.Mx = a.q[fs + c]; d.My = a.q[2 * fs + c]; d.Mz = a.q[3 * fs + c];
+    d.Bx = a.q[4 * fs + c]; d.By = a.q[5 * fs + c]; d.Bz = a.q[6 * fs + c];
+    d.E = a.q[7 * fs + c];
+    d.vx = __ddiv_rn(d.Mx, d.rho);
+    d.vy = __ddiv_rn(d.My, d.rho);
+    d.vz = __ddiv_rn(d.Mz, d.rho);
+    d.vv2 = __dadd_rn(__dadd_rn(__dmul_rn(d.vx, d.vx), __dmul_rn(d.vy, d.vy)), __dmul_rn(d.vz, d.vz));
+    d.BB2 = __dadd_rn(__dadd_rn(__dmul_rn(d.Bx, d.Bx), __dmul_rn(d.By, d.By)), __dmul_rn(d.Bz, d.Bz));
+    // (gam - 1) * (E - 0.5 * rho * vv2 - 0.5 * BB2), left to right
+    const double kin = __dmul_rn(__dmul_rn(0.5, d.rho), d.vv2);
+    d.pg = __dmul_rn(__dsub_rn(a.gam, 1.0), __dsub_rn(__dsub_rn(d.E, kin), __dmul_rn(0.5, d.BB2)));
+    // cell-centred central-difference divB: wrap when periodic, clamp when
+    // open (one-sided differences over d at a clamped edge)
+    double divB = 0.0;
+    if (g.nx > 1) {
+        const int im = out_bc_index(i - 1, 3, g.nx + 2, a.px), ip = out_bc_index(i + 1, 3, g.nx + 2, a.px);
+        const double diff = __dsub_rn(a.q[4 * fs + g.idx(ip, j, k)], a.q[4 * fs + g.idx(im, j, k)]);
+        divB = __dadd_rn(divB, __ddiv_rn(diff, (im == i || ip == i) ? a.dx : __dmul_rn(2.0, a.dx)));
+    }
+    if (g.ny > 1) {
+        const int jm = out_bc_index(j - 1, 3, g.ny + 2, a.py), jp = out_bc_index(j + 1, 3, g.ny + 2, a.py);
+        const double diff = __dsub_rn(a.q[5 * fs + g.idx(i, jp, k)], a.q[5 * fs + g.idx(i, jm, k)]);
+        divB = __dadd_rn(divB, __ddiv_rn(diff, (jm == j || jp == j) ? a.dy : __dmul_rn(2.0, a.dy)));
+    }
+    if (g.nz > 1) {
+        const int km = out_bc_index(k - 1, 3, g.nz + 2, a.pz), kp = out_bc_index(k + 1, 3, g.nz + 2, a.pz);
+        const double diff = __dsub_rn(a.q[6 * fs + g.idx(i, j, kp)], a.q[6 * fs + g.idx(i, j, km)]);
+        divB = __dadd_rn(divB, __ddiv_rn(diff, (km == k || kp == k) ? a.dz : __dmul_rn(2.0, a.dz)));
+    }
+    d.divB = divB;
+    return d;
+}
+
+// .vts slab: the ten appended arrays of src/output.cpp:380-395 in file order,
+// each holding this slab's points (x fastest): rho, pressure, energy, v2, B2,
+// divB (1 component), velocity, magnetic_field, momentum, points (3).
+constexpr int kVtsComps = 18;
+__global__ void k_dump_vts(DumpArgs a) {
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > a.g.nx + 2) return;
+    const int j = 3 + blockIdx.y, k = a.k0 + blockIdx.z;
+    const DumpCell d = dump_cell(a, i, j, k);
+    const long long n = (long long)a.g.nx * a.g.ny * a.nk;
+    const long long p = (i - 3) + (long long)a.g.nx * ((j - 3) + (long long)a.g.ny * (k - a.k0));
+    double* o = a.out;
+    o[p] = d.rho;
+    o[n + p] = d.pg;
+    o[2 * n + p] = d.E;
+    o[3 * n + p] = d.vv2;
+    o[4 * n + p] = d.BB2;
+    o[5 * n + p] = d.divB;
+    double* v = o + 6 * n + 3 * p;
+    v[0] = d.vx; v[1] = d.vy; v[2] = d.vz;
+    v += 3 * n;
+    v[0] = d.Bx; v[1] = d.By; v[2] = d.Bz;
+    v += 3 * n;
+    v[0] = d.Mx; v[1] = d.My; v[2] = d.Mz;
+    v += 3 * n;
+    v[0] = d.x; v[1] = d.y; v[2] = d.z;
+}
+
+// .dat slab: the 16 floating-point columns of a row (src/output.cpp:190-211)
+// per cell, cells in file order.
+constexpr int kDatCols = 16;
+__global__ void k_dump_dat(DumpArgs a) {
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > a.g.nx + 2) return;
+    const int j = 3 + blockIdx.y, k = a.k0 + blockIdx.z;
+    const DumpCell d = dump_cell(a, i, j, k);
+    const long long p = (i - 3) + (long long)a.g.nx * ((j - 3) + (long long)a.g.ny * (k - a.k0));
+    double* o = a.out + kDatCols * p;
+    o[0] = d.x; o[1] = d.y; o[2] = d.z;
+    o[3] = d.rho; o[4] = d.Mx; o[5] = d.My; o[6] = d.Mz;
+    o[7] = d.Bx; o[8] = d.By; o[9] = d.Bz; o[10] = d.E;
+    o[11] = d.pg; o[12] = d.vx; o[13] = d.vy; o[14] = d.vz; o[15] = d.divB;
+}
+
+// The stream's std::scientific, precision 15 rendering of a double.
+inline void put_sci(std::string& s, double v) {
+    char b[40];
+    const int n = std::snprintf(b, sizeof(b), "%.15e", v);
+    s.append(b, (size_t)n);
+}
+
+inline void put_int(std::string& s, long long v) {
+    char b[24];
+    const int n = std::snprintf(b, sizeof(b), "%lld", v);
+    s.append(b, (size_t)n);
+}
+
+// Full write of n bytes at offset off; false on an I/O error.
+bool pwrite_all(int fd, const void* data, size_t n, off_t off) {
+    const char* p = static_cast<const char*>(data);
+    while (n > 0) {
+        const ssize_t w = ::pwrite(fd, p, n, off);
+        if (w < 0) {
+            if (errno == EINTR) continue;
+            return false;
+        }
+        p += w; n -= (size_t)w; off += w;
+    }
+    return true;
+}
+
+// make_output_filename (src/output.cpp:21-38), serial form: <dir>/dumpNNNNNN<ext>
+std::string dump_name(const char* dir, int step, const char* ext) {
+    char b[32];
+    std::snprintf(b, sizeof(b), "dump%06d%s", step, ext);
+    std::string d = dir ? dir : "output";
+    return d.empty() ? std::string(b) : d + "/" + b;
+}
+
+int make_dirs(const std::string& dir) {
+    if (dir.empty()) return HOW_OK;
+    std::string cur;
+    for (size_t i = 0; i <= dir.size(); ++i) {
+        if (i == dir.size() || dir[i] == '/') {
+            if (!cur.empty() && ::mkdir(cur.c_str(), 0777) != 0 && errno != EEXIST) {
+                set_error("cannot create directory %s: %s", cur.c_str(), std::strerror(errno));
+                return HOW_ERR_ARG;
+            }
+        }
+        if (i < dir.size()) cur.push_back(dir[i]);
+    }
+    return HOW_OK;
+}
+
+// Planes per slab: the payload fits the staging buffer (8 fields) and at most
+// 2^26 doubles (512 MB) are held on the host at once.
+int slab_planes(const Ctx& c, int per_cell) {
+    const Grid& g = c.g;
+    const long long cap = std::min<long long>(8LL * g.fs, 1LL << 26);
+    long long k = cap / ((long long)per_cell * g.nx * g.ny);
+    if (k < 1) k = 1;
+    if (k > g.nz) k = g.nz;
+    return (int)k;
+}
+
+DumpArgs dump_args(const Ctx& c) {
+    DumpArgs a;
+    a.g = c.g;
+    a.q = c.q[0];
+    a.out = c.stage_buf;
+    a.k0 = 3; a.nk = 0;
+    a.px = c.p.bc[0] == HOW_BC_PERIODIC;
+    a.py = c.p.bc[1] == HOW_BC_PERIODIC;
+    a.pz = c.p.bc[2] == HOW_BC_PERIODIC;
+    a.dx = c.p.dx; a.dy = c.p.dy; a.dz = c.p.dz; a.gam = c.p.gam;
+    return a;
+}
+
+int copy_slab(Ctx& c, std::vector<double>& host, size_t n) {
+    host.resize(n);
+    HOW_CUDA_CHECK(cudaGetLastError());
+    HOW_CUDA_CHECK(cudaMemcpyAsync(host.data(), c.stage_buf, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    HOW_CUDA_CHECK(cudaStreamSynchronize(c.stream));
+    return HOW_OK;
+}
+
+int write_vts(Ctx& c, int step, double time, const std::string& path) {
+    const Grid& g = c.g;
+    const long long npts = (long long)g.nx * g.ny * g.nz;
+    // appended blocks: [u64 bytes][payload], offsets from the byte after "_"
+    const int ncomp[10] = {1, 1, 1, 1, 1, 1, 3, 3, 3, 3};
+    unsigned long long off[10], pos = 0;
+    for (int b = 0; b < 10; ++b) { off[b] = pos; pos += 8 + 8ULL * ncomp[b] * npts; }
+    const unsigned long long payload = pos;
+
+    std::string h;
+    h += "<?xml version=\"1.0\"?>\n";
+    h += "<VTKFile type=\"StructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" header_type=\"UInt64\">\n";
+    h += "  <StructuredGrid WholeExtent=\"0 "; put_int(h, g.nx - 1); h += " 0 "; put_int(h, g.ny - 1);
+    h += " 0 "; put_int(h, g.nz - 1); h += "\">\n";
+    h += "    <Piece Extent=\"0 "; put_int(h, g.nx - 1); h += " 0 "; put_int(h, g.ny - 1);
+    h += " 0 "; put_int(h, g.nz - 1); h += "\">\n";
+    h += "      <FieldData>\n";
+    h += "        <DataArray type=\"Float64\" Name=\"time\" NumberOfTuples=\"1\" format=\"ascii\">\n";
+    h += "          "; put_sci(h, time); h += "\n";
+    h += "        </DataArray>\n";
+    h += "        <DataArray type=\"Int32\" Name=\"step\" NumberOfTuples=\"1\" format=\"ascii\">\n";
+    h += "          "; put_int(h, step); h += "\n";
+    h += "        </DataArray>\n";
+    h += "        <DataArray type=\"Int32\" Name=\"rank\" NumberOfTuples=\"1\" format=\"ascii\">\n";
+    h += "          0\n";
+    h += "        </DataArray>\n";
+    h += "        <DataArray type=\"Int32\" Name=\"global_start_index\" NumberOfComponents=\"3\" "
+         "NumberOfTuples=\"1\" format=\"ascii\">\n";
+    h += "          0 0 0\n";
+    h += "        </DataArray>\n";
+    h += "      </FieldData>\n";
+    h += "      <PointData>\n";
+    const char* names[9] = {"rho", "pressure", "energy", "v2", "B2", "divB", "velocity", "magnetic_field",
+                            "momentum"};
+    for (int b = 0; b < 9; ++b) {
+        h += "        <DataArray type=\"Float64\" Name=\""; h += names[b];
+        h += "\" NumberOfComponents=\""; put_int(h, ncomp[b]);
+        h += "\" format=\"appended\" offset=\""; put_int(h, (long long)off[b]); h += "\"/>\n";
+    }
+    h += "      </PointData>\n";
+    h += "      <CellData>\n";
+    h += "      </CellData>\n";
+    h += "      <Points>\n";
+    h += "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"appended\" offset=\"";
+    put_int(h, (long long)off[9]); h += "\"/>\n";
+    h += "      </Points>\n";
+    h += "    </Piece>\n";
+    h += "  </StructuredGrid>\n";
+    h += "  <AppendedData encoding=\"raw\">\n";
+    h += "_";
+    const off_t base = (off_t)h.size();
+    const char* tail = "\n  </AppendedData>\n</VTKFile>\n";
+
+    const int fd = ::open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0666);
+    if (fd < 0) { set_error("cannot open output file %s: %s", path.c_str(), std::strerror(errno)); return HOW_ERR_ARG; }
+    bool ok = pwrite_all(fd, h.data(), h.size(), 0);
+    for (int b = 0; b < 10 && ok; ++b) {
+        const unsigned long long nbytes = 8ULL * ncomp[b] * npts;
+        ok = pwrite_all(fd, &nbytes, 8, base + (off_t)off[b]);
+    }
+    ok = ok && pwrite_all(fd, tail, std::strlen(tail), base + (off_t)payload);
+
+    DumpArgs a = dump_args(c);
+    const int K = slab_planes(c, kVtsComps);
+    std::vector<double> host;
+    int rc = HOW_OK;
+    for (int k0 = 0; k0 < g.nz && ok && rc == HOW_OK; k0 += K) {
+        a.k0 = 3 + k0;
+        a.nk = std::min(K, g.nz - k0);
+        const long long n = (long long)g.nx * g.ny * a.nk;
+        k_dump_vts<<<dim3((g.nx + 127) / 128, g.ny, a.nk), 128, 0, c.stream>>>(a);
+        ++c.launches;
+        rc = copy_slab(c, host, (size_t)(kVtsComps * n));
+        if (rc) break;
+        const long long first = (long long)g.nx * g.ny * k0;   // this slab's first point
+        const double* src = host.data();
+        for (int b = 0; b < 10 && ok; ++b) {
+            const off_t at = base + (off_t)off[b] + 8 + (off_t)(8LL * ncomp[b] * first);
+            ok = pwrite_all(fd, src, (size_t)(8LL * ncomp[b] * n), at);
+            src += ncomp[b] * n;
+        }
+    }
+    if (::close(fd) != 0) ok = false;
+    if (rc) return rc;
+    if (!ok) { set_error("write to %s failed: %s", path.c_str(), std::strerror(errno)); return HOW_ERR_ARG; }
+    return HOW_OK;
+}
+
+int write_dat(Ctx& c, int step, double time, const std::string& path) {
+    const Grid& g = c.g;
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) { set_error("cannot open output file %s: %s", path.c_str(), std::strerror(errno)); return HOW_ERR_ARG; }
+    std::string h;
+    h += "# step = "; put_int(h, step); h += "\n";
+    h += "# time = "; put_sci(h, time); h += "\n";
+    h += "# rank = 0\n";
+    h += "# local_active_size = "; put_int(h, g.nx); h += " "; put_int(h, g.ny); h += " "; put_int(h, g.nz); h += "\n";
+    h += "# global_active_size = "; put_int(h, g.nx); h += " "; put_int(h, g.ny); h += " "; put_int(h, g.nz);
+    h += "\n";
+    h += "# global_start_index = 0 0 0\n";
+    h += "# columns: ig jg kg il jl kl x y z rho Mx My Mz Bx By Bz E pg vx vy vz divB\n";
+    bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
+
+    DumpArgs a = dump_args(c);
+    const int K = slab_planes(c, kDatCols);
+    std::vector<double> host;
+    int rc = HOW_OK;
+    for (int k0 = 0; k0 < g.nz && ok && rc == HOW_OK; k0 += K) {
+        a.k0 = 3 + k0;
+        a.nk = std::min(K, g.nz - k0);
+        const long long n = (long long)g.nx * g.ny * a.nk;
+        k_dump_dat<<<dim3((g.nx + 127) / 128, g.ny, a.nk), 128, 0, c.stream>>>(a);
+        ++c.launches;
+        rc = copy_slab(c, host, (size_t)(kDatCols * n));
+        if (rc) break;
+        // one text row per (j, k) line of the slab, formatted in parallel
+        const int rows = g.ny * a.nk;
+        std::vector<std::string> text((size_t)rows);
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int r = 0; r < rows; ++r) {
+            const int jl = r % g.ny, kl = k0 + r / g.ny;
+            std::string& s = text[(size_t)r];
+            s.reserve((size_t)g.nx * 400);
+            for (int il = 0; il < g.nx; ++il) {
+                const double* v = host.data() + kDatCols * ((long long)r * g.nx + il);
+                put_int(s, il); s += ' '; put_int(s, jl); s += ' '; put_int(s, kl); s += ' ';
+                put_int(s, il); s += ' '; put_int(s, jl); s += ' '; put_int(s, kl);
+                for (int m = 0; m < kDatCols; ++m) { s += ' '; put_sci(s, v[m]); }
+                s += '\n';
+            }
+        }
+        for (int r = 0; r < rows && ok; ++r) ok = std::fwrite(text[r].data(), 1, text[r].size(), f) == text[r].size();
+    }
+    if (std::fclose(f) != 0) ok = false;
+    if (rc) return rc;
+    if (!ok) { set_error("write to %s failed", path.c_str()); return HOW_ERR_ARG; }
+    return HOW_OK;
+}
+
+}  // namespace
+}  // namespace how
+
+using namespace how;
+
+extern "C" int how_output(how_ctx* c, int step, double time, const char* dir) {
+    if (!c) { set_error("null context"); return HOW_ERR_ARG; }
+    HOW_CUDA_CHECK(cudaSetDevice(c->dev));
+    const std::string fmt = c->p.output_format;
+    const bool dat = fmt == "dat", vts = fmt == "vtk" || fmt == "vts";
+    if (!dat && !vts) {
+        // the reference prints the options and aborts (src/output.cpp:566-570)
+        set_error("unknown output_format = %s (available options: dat, vtk)", fmt.c_str());
+        return HOW_ERR_ARG;
+    }
+    const std::string d = dir ? dir : "output";
+    int rc = make_dirs(d);
+    if (rc) return rc;
+    const std::string path = dump_name(dir, step, dat ? ".dat" : ".vts");
+    HOW_CUDA_CHECK(cudaStreamSynchronize(c->stream));   // q(0) final
+    return dat ? write_dat(*c, step, time, path) : write_vts(*c, step, time, path);
+}

@@ -99,6 +99,7 @@ def _load():
         "how_sweep": ([V, ctypes.c_int, ctypes.c_double], ctypes.c_int),
         "how_get_ct_array": ([V, ctypes.c_int, D], ctypes.c_int),
         "how_run": ([V, D, ctypes.c_long, ctypes.POINTER(ctypes.c_long), D, ctypes.c_long], ctypes.c_int),
+        "how_output": ([V, ctypes.c_int, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
         "how_set_precision": ([V, ctypes.c_int], ctypes.c_int),
         "how_sync": ([V], ctypes.c_int),
         "how_kernel_launches": ([V], ctypes.c_long),
@@ -339,6 +340,19 @@ class Domain:
         dts = np.zeros(max(dts_cap, 1))
         _check(_lib.how_run(self._h, ctypes.byref(t), max_steps, ctypes.byref(s), _dptr(dts), dts_cap))
         return t.value, s.value, dts[: min(s.value, dts_cap)].copy()
+
+    def output(self, step, time, directory=None):
+        """Write the dump file of q(0) in the parameters' output_format, as
+        the reference's output(q, par, step, time) (src/output.cpp:555-572):
+        <directory>/dumpNNNNNN.dat or .vts, directory "output" by default.
+        Returns the file's path."""
+        d = "output" if directory is None else str(directory)
+        _check(_lib.how_output(self._h, int(step), float(time), d.encode()))
+        fmt = self.params.output_format.decode() if isinstance(self.params.output_format, bytes) \
+            else str(self.params.output_format)
+        ext = ".dat" if fmt == "dat" else ".vts"
+        name = "dump%06d%s" % (int(step), ext)
+        return name if d == "" else d + "/" + name
 
     def sweep_phase_profile(self, direction: int, dt: float):
         """Mean cycles per block of each sweep phase (instrumentation)."""

@@ -150,6 +150,19 @@ int how_get_ct_array(how_ctx* ctx, int which, double* host);
  * Updates *time and *steps.  dts (may be NULL) receives each step's dt. */
 int how_run(how_ctx* ctx, double* time, long max_steps, long* steps, double* dts, long dts_cap);
 
+/* Dump file of q(0), output() (src/output.cpp:555-572), in the context's
+ * output_format: "dat" -> <dir>/dumpNNNNNN.dat, the ASCII table of
+ * output_dat (src/output.cpp:65-224); "vtk" or "vts" -> <dir>/dumpNNNNNN.vts,
+ * the binary appended-raw StructuredGrid of output_vts_binary
+ * (src/output.cpp:226-552).  dir NULL means "output", the reference's
+ * directory; it is created if missing.  The derived columns (velocity, gas
+ * pressure, v^2, B^2, the cell-centred divB diagnostic, coordinates) are
+ * formed on the device and the files equal the reference's byte for byte.
+ * An unknown format returns HOW_ERR_ARG where the reference aborts.  The
+ * call returns once the file is written; it stages the data through the
+ * context's own buffer, one slab of z planes at a time. */
+int how_output(how_ctx* ctx, int step, double time, const char* dir);
+
 /* How the sweeps compute (HOW_PREC_*). */
 int how_set_precision(how_ctx* ctx, int mode);
 

@@ -2,7 +2,7 @@
 // TEST INFRASTRUCTURE ONLY (the checker, never the product).
 //
 // Built by oracle/Makefile together with the reference's src/*.cpp (minus
-// main.cpp and output.cpp) against the project-written Kokkos shim in
+// main.cpp) against the project-written Kokkos shim in
 // oracle/kokkos_shim/.  It reproduces the reference driver's set-up
 // (src/main.cpp:84-130) and time loop (src/main.cpp:158-223), and dumps raw
 // state so the tests can compare the B200 path with the reference's own
@@ -11,6 +11,7 @@
 // usage:
 //   how_ref <input.in> <out.bin> [--steps K] [--state in.bin] [--dump-stages]
 //           [--sweep x|y|z --dt DT] [--threads N] [--time-only]
+//           [--output STEP TIME]
 //
 //   default      : main-loop semantics (tstep, dt clamp to the output time,
 //                  ssprk) until tend, or until K hydro steps when --steps K.
@@ -22,6 +23,10 @@
 //   --sweep d    : only stage iw=1's copy/bound and ONE directional sweep with
 //                  the given dt; dumps q(1) and the two CT flux arrays it fills.
 //   --time-only  : no dump; prints wall seconds and zone-cycles/s as JSON.
+//   --output S T : only the reference's own output(q, par, S, T)
+//                  (src/output.cpp:555-572) on the initial or --state q(0):
+//                  output/dumpSSSSSS.dat or .vts in the working directory, in
+//                  the input's output_format.  <out.bin> is not written.
 //
 // Dump format: a sequence of records
 //   u32 name_len, name bytes, u32 ndim, u64 dims[ndim], f64 data[prod(dims)]
@@ -36,6 +41,7 @@
 #include "fluxct.hpp"
 #include "bound.hpp"
 #include "prot.hpp"
+#include "output.hpp"
 
 #include <cmath>
 #include <cstdint>
@@ -180,7 +186,9 @@ int main(int argc, char** argv) {
     long max_steps = -1, warmup = 0;
     std::string state_path, sweep;
     double sweep_dt = 0.0;
-    bool dump_stages = false, time_only = false;
+    bool dump_stages = false, time_only = false, do_output = false;
+    int out_step = 0;
+    double out_time = 0.0;
     for (int a = 3; a < argc; ++a) {
         std::string s = argv[a];
         if (s == "--steps" && a + 1 < argc) max_steps = std::atol(argv[++a]);
@@ -191,6 +199,11 @@ int main(int argc, char** argv) {
         else if (s == "--threads" && a + 1 < argc) omp_set_num_threads(std::atoi(argv[++a]));
         else if (s == "--time-only") time_only = true;
         else if (s == "--warmup" && a + 1 < argc) warmup = std::atol(argv[++a]);
+        else if (s == "--output" && a + 2 < argc) {
+            do_output = true;
+            out_step = std::atoi(argv[++a]);
+            out_time = std::atof(argv[++a]);
+        }
         else { std::fprintf(stderr, "unknown option %s\n", s.c_str()); return 2; }
     }
 
@@ -241,7 +254,9 @@ int main(int argc, char** argv) {
             initialize_bfield_from_q(q, par);   // src/main.cpp:130
         }
 
-        if (!sweep.empty()) {
+        if (do_output) {
+            output(q, par, out_step, out_time);   // src/output.cpp:555-572
+        } else if (!sweep.empty()) {
             Writer w(out);
             dump_state(w, "init_", q, 0, par);
             CTFluxes ct(par);
