@@ -209,6 +209,7 @@ int how_create(const how_params* p, how_ctx** out) {
 int how_destroy(how_ctx* c) {
     if (!c) return HOW_OK;
     cudaSetDevice(c->dev);
+    dump_release(*c);   // an asynchronous dump still being written finishes first
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->mem) cudaFree(c->mem);
     if (c->router_w) cudaFree(c->router_w);

@@ -170,6 +170,7 @@ struct Ctx {
     float route_thr = 0.0f, guard_jump = 0.25f, guard_floor = 100.0f;
     int route_refresh = 5;                // learned routing: fresh decisions every this many stages (1..5)
     int cur_stage = 1;                    // SSPRK stage being launched (1..5)
+    struct DumpJob* dump = nullptr;       // asynchronous dump file in flight (output.cu)
 };
 
 // ---- kernels / launchers (defined in the .cu files) ------------------------
@@ -188,6 +189,9 @@ void launch_prot(Ctx& c, int stage);
 void launch_stage5_base(Ctx& c, double c4, double c5);
 int make_sweep_tensor_maps(Ctx& c);
 void launch_copy_fields(Ctx& c, double* dst, const double* src, int nfields);
+
+// asynchronous dump files (output.cu): join the writer, free its buffers
+void dump_release(Ctx& c);
 
 void set_error(const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);

@@ -11,6 +11,11 @@
 // and written: the .vts blocks at their final file offsets (pwrite), the .dat
 // lines formatted by host threads.  Only the file assembly is host code.
 //
+// how_output_async forms the whole domain's payload into its own HBM buffer
+// on the main stream, copies it into pinned host memory on a side stream and
+// writes the file from a host thread, so the steps queued after it overlap
+// the copy and the write; how_output_wait joins the writer.
+//
 // The values are the reference's bit for bit: every operation is a separately
 // rounded IEEE operation in the reference's evaluation order (the _rn
 // intrinsics, which the compiler never fuses into FMAs), and the text uses
@@ -25,7 +30,9 @@
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace how {
@@ -217,16 +224,11 @@ DumpArgs dump_args(const Ctx& c) {
     return a;
 }
 
-int copy_slab(Ctx& c, std::vector<double>& host, size_t n) {
-    host.resize(n);
-    HOW_CUDA_CHECK(cudaGetLastError());
-    HOW_CUDA_CHECK(cudaMemcpyAsync(host.data(), c.stage_buf, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    HOW_CUDA_CHECK(cudaStreamSynchronize(c.stream));
-    return HOW_OK;
-}
+// Supplies the payload of active planes [k0, k0 + nk) in the kernels' slab
+// layout, host-resident.
+using SlabFn = std::function<int(int k0, int nk, const double** data)>;
 
-int write_vts(Ctx& c, int step, double time, const std::string& path) {
-    const Grid& g = c.g;
+int assemble_vts(const Grid& g, int step, double time, const std::string& path, int K, const SlabFn& slab) {
     const long long npts = (long long)g.nx * g.ny * g.nz;
     // appended blocks: [u64 bytes][payload], offsets from the byte after "_"
     const int ncomp[10] = {1, 1, 1, 1, 1, 1, 3, 3, 3, 3};
@@ -286,21 +288,14 @@ int write_vts(Ctx& c, int step, double time, const std::string& path) {
         ok = pwrite_all(fd, &nbytes, 8, base + (off_t)off[b]);
     }
     ok = ok && pwrite_all(fd, tail, std::strlen(tail), base + (off_t)payload);
-
-    DumpArgs a = dump_args(c);
-    const int K = slab_planes(c, kVtsComps);
-    std::vector<double> host;
     int rc = HOW_OK;
     for (int k0 = 0; k0 < g.nz && ok && rc == HOW_OK; k0 += K) {
-        a.k0 = 3 + k0;
-        a.nk = std::min(K, g.nz - k0);
-        const long long n = (long long)g.nx * g.ny * a.nk;
-        k_dump_vts<<<dim3((g.nx + 127) / 128, g.ny, a.nk), 128, 0, c.stream>>>(a);
-        ++c.launches;
-        rc = copy_slab(c, host, (size_t)(kVtsComps * n));
+        const int nk = std::min(K, g.nz - k0);
+        const long long n = (long long)g.nx * g.ny * nk;
+        const double* src = nullptr;
+        rc = slab(k0, nk, &src);
         if (rc) break;
         const long long first = (long long)g.nx * g.ny * k0;   // this slab's first point
-        const double* src = host.data();
         for (int b = 0; b < 10 && ok; ++b) {
             const off_t at = base + (off_t)off[b] + 8 + (off_t)(8LL * ncomp[b] * first);
             ok = pwrite_all(fd, src, (size_t)(8LL * ncomp[b] * n), at);
@@ -313,8 +308,7 @@ int write_vts(Ctx& c, int step, double time, const std::string& path) {
     return HOW_OK;
 }
 
-int write_dat(Ctx& c, int step, double time, const std::string& path) {
-    const Grid& g = c.g;
+int assemble_dat(const Grid& g, int step, double time, const std::string& path, int K, const SlabFn& slab) {
     std::FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) { set_error("cannot open output file %s: %s", path.c_str(), std::strerror(errno)); return HOW_ERR_ARG; }
     std::string h;
@@ -327,21 +321,14 @@ int write_dat(Ctx& c, int step, double time, const std::string& path) {
     h += "# global_start_index = 0 0 0\n";
     h += "# columns: ig jg kg il jl kl x y z rho Mx My Mz Bx By Bz E pg vx vy vz divB\n";
     bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
-
-    DumpArgs a = dump_args(c);
-    const int K = slab_planes(c, kDatCols);
-    std::vector<double> host;
     int rc = HOW_OK;
     for (int k0 = 0; k0 < g.nz && ok && rc == HOW_OK; k0 += K) {
-        a.k0 = 3 + k0;
-        a.nk = std::min(K, g.nz - k0);
-        const long long n = (long long)g.nx * g.ny * a.nk;
-        k_dump_dat<<<dim3((g.nx + 127) / 128, g.ny, a.nk), 128, 0, c.stream>>>(a);
-        ++c.launches;
-        rc = copy_slab(c, host, (size_t)(kDatCols * n));
+        const int nk = std::min(K, g.nz - k0);
+        const double* src = nullptr;
+        rc = slab(k0, nk, &src);
         if (rc) break;
         // one text row per (j, k) line of the slab, formatted in parallel
-        const int rows = g.ny * a.nk;
+        const int rows = g.ny * nk;
         std::vector<std::string> text((size_t)rows);
 #pragma omp parallel for schedule(dynamic, 4)
         for (int r = 0; r < rows; ++r) {
@@ -349,7 +336,7 @@ int write_dat(Ctx& c, int step, double time, const std::string& path) {
             std::string& s = text[(size_t)r];
             s.reserve((size_t)g.nx * 400);
             for (int il = 0; il < g.nx; ++il) {
-                const double* v = host.data() + kDatCols * ((long long)r * g.nx + il);
+                const double* v = src + kDatCols * ((long long)r * g.nx + il);
                 put_int(s, il); s += ' '; put_int(s, jl); s += ' '; put_int(s, kl); s += ' ';
                 put_int(s, il); s += ' '; put_int(s, jl); s += ' '; put_int(s, kl);
                 for (int m = 0; m < kDatCols; ++m) { s += ' '; put_sci(s, v[m]); }
@@ -364,25 +351,161 @@ int write_dat(Ctx& c, int step, double time, const std::string& path) {
     return HOW_OK;
 }
 
+void launch_dump(Ctx& c, DumpArgs a, bool dat) {
+    const dim3 grid((c.g.nx + 127) / 128, c.g.ny, a.nk);
+    if (dat) k_dump_dat<<<grid, 128, 0, c.stream>>>(a);
+    else k_dump_vts<<<grid, 128, 0, c.stream>>>(a);
+    ++c.launches;
+}
+
+// Checks the context and the format; *skip when output_format is "none".
+int dump_prologue(how_ctx* c, const char* dir, bool* dat, bool* skip, std::string* path, int step) {
+    if (!c) { set_error("null context"); return HOW_ERR_ARG; }
+    HOW_CUDA_CHECK(cudaSetDevice(c->dev));
+    const std::string fmt = c->p.output_format;
+    *skip = fmt == "none";
+    if (*skip) return HOW_OK;
+    *dat = fmt == "dat";
+    if (!*dat && fmt != "vtk" && fmt != "vts") {
+        // the reference prints the options and aborts (src/output.cpp:566-570)
+        set_error("unknown output_format = %s (available options: dat, vtk, none)", fmt.c_str());
+        return HOW_ERR_ARG;
+    }
+    const int rc = make_dirs(dir ? dir : "output");
+    if (rc) return rc;
+    *path = dump_name(dir, step, *dat ? ".dat" : ".vts");
+    return HOW_OK;
+}
+
 }  // namespace
+
+// Asynchronous dumps: the payload of the whole domain in HBM, copied on a side
+// stream into pinned host memory once the main stream has formed it, and
+// written by a host thread.  One dump is in flight per context.
+struct DumpJob {
+    double* dev = nullptr;
+    size_t dev_n = 0;
+    double* host = nullptr;
+    size_t host_n = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t formed = nullptr, copied = nullptr;
+    std::thread writer;
+    bool busy = false;
+    int rc = HOW_OK;
+    std::string err;
+};
+
+int dump_join(Ctx& c) {
+    DumpJob* j = c.dump;
+    if (!j || !j->busy) return HOW_OK;
+    j->writer.join();
+    j->busy = false;
+    if (j->rc) set_error("%s", j->err.c_str());
+    return j->rc;
+}
+
+void dump_release(Ctx& c) {
+    if (!c.dump) return;
+    dump_join(c);
+    DumpJob* j = c.dump;
+    if (j->dev) cudaFree(j->dev);
+    if (j->host) cudaFreeHost(j->host);
+    if (j->formed) cudaEventDestroy(j->formed);
+    if (j->copied) cudaEventDestroy(j->copied);
+    if (j->side) cudaStreamDestroy(j->side);
+    delete j;
+    c.dump = nullptr;
+}
+
 }  // namespace how
 
 using namespace how;
 
 extern "C" int how_output(how_ctx* c, int step, double time, const char* dir) {
-    if (!c) { set_error("null context"); return HOW_ERR_ARG; }
-    HOW_CUDA_CHECK(cudaSetDevice(c->dev));
-    const std::string fmt = c->p.output_format;
-    const bool dat = fmt == "dat", vts = fmt == "vtk" || fmt == "vts";
-    if (!dat && !vts) {
-        // the reference prints the options and aborts (src/output.cpp:566-570)
-        set_error("unknown output_format = %s (available options: dat, vtk)", fmt.c_str());
-        return HOW_ERR_ARG;
-    }
-    const std::string d = dir ? dir : "output";
-    int rc = make_dirs(d);
-    if (rc) return rc;
-    const std::string path = dump_name(dir, step, dat ? ".dat" : ".vts");
+    bool dat = false, skip = false;
+    std::string path;
+    int rc = dump_prologue(c, dir, &dat, &skip, &path, step);
+    if (rc || skip) return rc;
     HOW_CUDA_CHECK(cudaStreamSynchronize(c->stream));   // q(0) final
-    return dat ? write_dat(*c, step, time, path) : write_vts(*c, step, time, path);
+    DumpArgs a = dump_args(*c);
+    const int K = slab_planes(*c, dat ? kDatCols : kVtsComps);
+    std::vector<double> host;
+    Ctx& cx = *c;
+    SlabFn slab = [&](int k0, int nk, const double** data) -> int {
+        a.k0 = 3 + k0;
+        a.nk = nk;
+        launch_dump(cx, a, dat);
+        const size_t n = (size_t)(dat ? kDatCols : kVtsComps) * cx.g.nx * cx.g.ny * nk;
+        host.resize(n);
+        HOW_CUDA_CHECK(cudaGetLastError());
+        HOW_CUDA_CHECK(cudaMemcpyAsync(host.data(), cx.stage_buf, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                       cx.stream));
+        HOW_CUDA_CHECK(cudaStreamSynchronize(cx.stream));
+        *data = host.data();
+        return HOW_OK;
+    };
+    return dat ? assemble_dat(c->g, step, time, path, K, slab) : assemble_vts(c->g, step, time, path, K, slab);
+}
+
+extern "C" int how_output_async(how_ctx* c, int step, double time, const char* dir) {
+    bool dat = false, skip = false;
+    std::string path;
+    int rc = dump_prologue(c, dir, &dat, &skip, &path, step);
+    if (rc || skip) return rc;
+    if ((rc = dump_join(*c))) return rc;   // the previous dump first
+    if (!c->dump) c->dump = new DumpJob();
+    DumpJob* j = c->dump;
+    const Grid& g = c->g;
+    const size_t n = (size_t)(dat ? kDatCols : kVtsComps) * g.nx * g.ny * g.nz;
+    if (j->dev_n < n) {
+        if (j->dev) cudaFree(j->dev);
+        j->dev = nullptr; j->dev_n = 0;
+        HOW_CUDA_CHECK(cudaMalloc(&j->dev, n * sizeof(double)));
+        j->dev_n = n;
+    }
+    if (j->host_n < n) {
+        if (j->host) cudaFreeHost(j->host);
+        j->host = nullptr; j->host_n = 0;
+        HOW_CUDA_CHECK(cudaMallocHost(&j->host, n * sizeof(double)));
+        j->host_n = n;
+    }
+    if (!j->side) HOW_CUDA_CHECK(cudaStreamCreateWithFlags(&j->side, cudaStreamNonBlocking));
+    if (!j->formed) HOW_CUDA_CHECK(cudaEventCreateWithFlags(&j->formed, cudaEventDisableTiming));
+    if (!j->copied) HOW_CUDA_CHECK(cudaEventCreateWithFlags(&j->copied, cudaEventDisableTiming));
+    // the whole domain as one slab, ordered after the steps already queued
+    DumpArgs a = dump_args(*c);
+    a.out = j->dev;
+    a.k0 = 3;
+    a.nk = g.nz;
+    launch_dump(*c, a, dat);
+    HOW_CUDA_CHECK(cudaGetLastError());
+    HOW_CUDA_CHECK(cudaEventRecord(j->formed, c->stream));
+    HOW_CUDA_CHECK(cudaStreamWaitEvent(j->side, j->formed, 0));
+    HOW_CUDA_CHECK(cudaMemcpyAsync(j->host, j->dev, n * sizeof(double), cudaMemcpyDeviceToHost, j->side));
+    HOW_CUDA_CHECK(cudaEventRecord(j->copied, j->side));
+    j->rc = HOW_OK;
+    j->err.clear();
+    const int dev = c->dev;
+    const Grid gg = g;
+    j->writer = std::thread([j, dev, gg, step, time, path, dat]() {
+        int r = HOW_OK;
+        cudaError_t e = cudaSetDevice(dev);
+        if (e == cudaSuccess) e = cudaEventSynchronize(j->copied);
+        if (e != cudaSuccess) {
+            r = cuda_fail(e, "dump copy");
+        } else {
+            const double* host = j->host;
+            SlabFn whole = [host](int, int, const double** data) -> int { *data = host; return HOW_OK; };
+            r = dat ? assemble_dat(gg, step, time, path, gg.nz, whole) : assemble_vts(gg, step, time, path, gg.nz, whole);
+        }
+        j->rc = r;
+        if (r) j->err = how_last_error();
+    });
+    j->busy = true;
+    return HOW_OK;
+}
+
+extern "C" int how_output_wait(how_ctx* c) {
+    if (!c) { set_error("null context"); return HOW_ERR_ARG; }
+    return dump_join(*c);
 }

@@ -100,6 +100,8 @@ def _load():
         "how_get_ct_array": ([V, ctypes.c_int, D], ctypes.c_int),
         "how_run": ([V, D, ctypes.c_long, ctypes.POINTER(ctypes.c_long), D, ctypes.c_long], ctypes.c_int),
         "how_output": ([V, ctypes.c_int, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
+        "how_output_async": ([V, ctypes.c_int, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
+        "how_output_wait": ([V], ctypes.c_int),
         "how_set_precision": ([V, ctypes.c_int], ctypes.c_int),
         "how_sync": ([V], ctypes.c_int),
         "how_kernel_launches": ([V], ctypes.c_long),
@@ -341,18 +343,31 @@ class Domain:
         _check(_lib.how_run(self._h, ctypes.byref(t), max_steps, ctypes.byref(s), _dptr(dts), dts_cap))
         return t.value, s.value, dts[: min(s.value, dts_cap)].copy()
 
+    def _dump_path(self, step, d):
+        fmt = self.params.output_format.decode() if isinstance(self.params.output_format, bytes) \
+            else str(self.params.output_format)
+        if fmt == "none":
+            return None
+        name = "dump%06d%s" % (int(step), ".dat" if fmt == "dat" else ".vts")
+        return name if d == "" else d + "/" + name
+
     def output(self, step, time, directory=None):
         """Write the dump file of q(0) in the parameters' output_format, as
         the reference's output(q, par, step, time) (src/output.cpp:555-572):
         <directory>/dumpNNNNNN.dat or .vts, directory "output" by default.
-        Returns the file's path."""
+        Returns the file's path (None for output_format none)."""
         d = "output" if directory is None else str(directory)
         _check(_lib.how_output(self._h, int(step), float(time), d.encode()))
-        fmt = self.params.output_format.decode() if isinstance(self.params.output_format, bytes) \
-            else str(self.params.output_format)
-        ext = ".dat" if fmt == "dat" else ".vts"
-        name = "dump%06d%s" % (int(step), ext)
-        return name if d == "" else d + "/" + name
+        return self._dump_path(step, d)
+
+    def output_async(self, step, time, directory=None):
+        """The same dump, written while later steps run; output_wait() joins."""
+        d = "output" if directory is None else str(directory)
+        _check(_lib.how_output_async(self._h, int(step), float(time), d.encode()))
+        return self._dump_path(step, d)
+
+    def output_wait(self):
+        _check(_lib.how_output_wait(self._h))
 
     def sweep_phase_profile(self, direction: int, dt: float):
         """Mean cycles per block of each sweep phase (instrumentation)."""

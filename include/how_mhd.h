@@ -158,10 +158,25 @@ int how_run(how_ctx* ctx, double* time, long max_steps, long* steps, double* dts
  * directory; it is created if missing.  The derived columns (velocity, gas
  * pressure, v^2, B^2, the cell-centred divB diagnostic, coordinates) are
  * formed on the device and the files equal the reference's byte for byte.
- * An unknown format returns HOW_ERR_ARG where the reference aborts.  The
+ * An unknown format returns HOW_ERR_ARG where the reference aborts;
+ * output_format "none" (a mode the reference lists as a to-do) writes
+ * nothing.  The
  * call returns once the file is written; it stages the data through the
  * context's own buffer, one slab of z planes at a time. */
 int how_output(how_ctx* ctx, int step, double time, const char* dir);
+
+/* The same dump, without waiting for it: the derived columns of the whole
+ * domain are formed into a device buffer on the context's stream (ordered
+ * after the steps already queued), copied into pinned host memory on a side
+ * stream, and written by a host thread, so steps queued next run while the
+ * file is copied and written.  One dump is in flight per context; a second
+ * call first waits for the previous one.  The buffers (18 doubles per cell
+ * for .vts, 16 for .dat, on the device and pinned on the host) are kept for
+ * reuse until how_destroy.  output_format "none" writes nothing (also for
+ * how_output). */
+int how_output_async(how_ctx* ctx, int step, double time, const char* dir);
+/* Waits for the dump in flight, if any; returns its status. */
+int how_output_wait(how_ctx* ctx);
 
 /* How the sweeps compute (HOW_PREC_*). */
 int how_set_precision(how_ctx* ctx, int mode);

@@ -85,3 +85,45 @@ def test_unknown_format_is_an_error(tmp_path):
         d.init_problem()
         with pytest.raises(hm.HowError):
             d.output(0, 0.0, tmp_path)
+
+
+@pytest.mark.parametrize("fmt", ["vts", "dat"])
+def test_async_dump_overlaps_the_steps(tmp_path, fmt):
+    """how_output_async of a state, then three steps while it is written:
+    the file equals the synchronous dump of that state, and the steps equal
+    a run without dumps, bit for bit."""
+    import how_mhd as hm
+    kw = dict(nx=40, ny=36, nz=32, nt=1, tend=100.0, gam=5.0 / 3.0, cour=0.4, problem="blast3d_b",
+              rhomin=1e-6, pgmin=1e-6, output_format=fmt)
+    p = hm.make_parameters(**kw)
+    with hm.Domain(p) as d:
+        d.init_problem()
+        t, _, _ = d.run(0.0, 2)
+        sync = Path(d.output(2, t, tmp_path / "sync"))
+        path = Path(d.output_async(2, t, tmp_path / "async"))
+        d.run(t, 3)
+        d.output_wait()
+        q = d.get_state(0)
+        # a second dump reuses the buffers
+        again = Path(d.output_async(5, 1.0, tmp_path / "again"))
+        d.output_wait()
+    with hm.Domain(p) as d:
+        d.init_problem()
+        t, _, _ = d.run(0.0, 2)
+        d.run(t, 3)
+        q_ref = d.get_state(0)
+        ref5 = Path(d.output(5, 1.0, tmp_path / "ref5"))
+    assert path.read_bytes() == sync.read_bytes()
+    np.testing.assert_array_equal(q, q_ref)
+    assert again.read_bytes() == ref5.read_bytes()
+
+
+def test_format_none_writes_nothing(tmp_path):
+    import how_mhd as hm
+    p = hm.make_parameters(nx=8, ny=8, nz=1, nt=1, tend=0.1, problem="orszag_tang", output_format="none")
+    with hm.Domain(p) as d:
+        d.init_problem()
+        assert d.output(0, 0.0, tmp_path / "o") is None
+        assert d.output_async(1, 0.0, tmp_path / "o") is None
+        d.output_wait()
+    assert not (tmp_path / "o").exists()
