@@ -232,7 +232,7 @@ int how_ensemble_member_status(const how_ensemble* e, int m, double* time, long*
 long how_ensemble_graph_launches(const how_ensemble* e);
 
 /* ------------------------------------------------------- learned routing */
-/* No counterpart in the reference (the north star's learned part).  A
+/* No counterpart in the reference (an addition of this library).  A
  * 6 -> 32 -> 32 -> 1 GELU network, packed FP32 as W1[32][6], b1[32],
  * W2[32][32], b2[32], w3[32], b3 (how_router_param_count() floats), routes
  * each interface of each sweep to the full characteristic WENO5 or to a
