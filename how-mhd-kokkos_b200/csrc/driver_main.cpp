@@ -1,9 +1,12 @@
 // driver_main.cpp -- how_mhd_b200: the driver of src/main.cpp:25-248 on the
 // C ABI.  Reads input.in (argv[1] or stdin), initialises the registered
 // problem, and advances through the nt output intervals with the reference's
-// dt clamp, logging one line per interval.  File output (.dat/.vts) is not
-// part of this path; --dump FILE writes the final q(0) in the reference
-// layout as raw doubles.
+// dt clamp, logging one line per interval.  Like the reference it writes a
+// dump file of the initial state and of each interval's end
+// (src/main.cpp:144, 225) into output/, in the input's output_format
+// ("none" skips them); each dump is written while the next interval runs.
+// --dump FILE also writes the final q(0) in the reference layout as raw
+// doubles.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -39,6 +42,11 @@ int main(int argc, char** argv) {
     double time = 0.0;
     long total = 0;
     const double dtout = p.tend / (double)p.nt;
+    if ((rc = how_output_async(ctx, 0, time, "output"))) {
+        std::fprintf(stderr, "Error: %s\n", how_last_error());
+        how_destroy(ctx);
+        return 1;
+    }
     std::printf("dtout = %g\noutput step = 0 time = 0\n", dtout);
     for (int out = 1; out <= p.nt; ++out) {
         // run one output interval: how_run stops at the interval end because
@@ -59,9 +67,15 @@ int main(int argc, char** argv) {
         }
         total += steps;
         if (rc) { std::fprintf(stderr, "Error: %s\n", how_last_error()); break; }
+        if ((rc = how_output_async(ctx, out, time, "output"))) {
+            std::fprintf(stderr, "Error: %s\n", how_last_error());
+            break;
+        }
         std::printf("output step = %d time = %.10g last_dt = %.6g hydro_steps = %ld\n", out, time,
                     dts[0], steps);
     }
+    const int wrc = how_output_wait(ctx);
+    if (wrc) { std::fprintf(stderr, "Error: %s\n", how_last_error()); rc = wrc; }
     if (!dump.empty()) {
         std::vector<double> qh((size_t)8 * (p.nx + 6) * (p.ny + 6) * (p.nz + 6));
         if (how_get_state(ctx, 0, qh.data()) == HOW_OK) {
