@@ -127,3 +127,21 @@ def test_format_none_writes_nothing(tmp_path):
         assert d.output_async(1, 0.0, tmp_path / "o") is None
         d.output_wait()
     assert not (tmp_path / "o").exists()
+
+
+def test_driver_writes_the_reference_dumps(tmp_path):
+    """how_mhd_b200 writes output/dump000000 (the initial state, which equals
+    the reference's initial condition bit for bit) and one dump per output
+    interval; the initial one is the file the reference's driver writes."""
+    exe = REF_BIN.parents[2] / "how-mhd-kokkos_b200" / "how_mhd_b200"
+    kw = dict(nx=32, ny=32, nz=1, nt=2, tend=0.02, gam=5.0 / 3.0, cour=0.4, problem="orszag_tang",
+              x1bc="periodic", x2bc="periodic", x3bc="periodic", output_format="vts")
+    inp = write_input(tmp_path / "in.in", **kw)
+    run = tmp_path / "ours"
+    run.mkdir()
+    subprocess.run([str(exe), str(inp)], cwd=run, check=True, capture_output=True, timeout=300)
+    for s in range(3):
+        assert (run / "output" / f"dump{s:06d}.vts").exists()
+    subprocess.run([str(REF_BIN), str(inp), "/dev/null", "--output", "0", "0.0"], cwd=tmp_path, check=True,
+                   capture_output=True, timeout=300)
+    assert (run / "output" / "dump000000.vts").read_bytes() == (tmp_path / "output" / "dump000000.vts").read_bytes()
