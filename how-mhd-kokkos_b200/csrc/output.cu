@@ -200,8 +200,9 @@ int make_dirs(const std::string& dir) {
     return HOW_OK;
 }
 
-// Planes per slab: the payload fits the staging buffer (8 fields) and at most
-// 2^26 doubles (512 MB) are held on the host at once.
+// Planes per slab: the payload fits the staging buffer (8 fields, always room
+// for one plane's 18 values per cell) and, unless a single plane is larger,
+// at most 2^26 doubles (512 MB) are held on the host at once.
 int slab_planes(const Ctx& c, int per_cell) {
     const Grid& g = c.g;
     const long long cap = std::min<long long>(8LL * g.fs, 1LL << 26);
