@@ -56,20 +56,28 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--n", type=int, default=None, help="cells per axis (default 256; 384 for --workload turbulence)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--t-start", type=float, default=0.05,
                     help="simulated time the timed steps start from (the blast evolved there first)")
     ap.add_argument("--no-fast", action="store_true", help="skip the mixed-precision + learned-routing leg")
-    ap.add_argument("--workload", default="blast", choices=["blast", "ensemble", "accuracy", "output"],
+    ap.add_argument("--workload", default="blast", choices=["blast", "ensemble", "accuracy", "output", "turbulence"],
                     help="ensemble: 64 uneven 2-D/1-D runs batched vs advanced one by one; "
                          "accuracy: whole blast run to --tend in every precision / routing form; "
-                         "output: dump files (how_output) of the blast state, .vts and .dat")
+                         "output: dump files (how_output) of the blast state, .vts and .dat; "
+                         "turbulence: learned routing on decaying turbulence (turb3d, --n 384)")
     ap.add_argument("--out-dir", default="/tmp/how_dumps", help="--workload output: where the dumps go")
     ap.add_argument("--tend", type=float, default=0.2, help="end time of --workload accuracy")
     ap.add_argument("--forms", default="",
                     help="--workload accuracy: ';'-separated subset of the forms after fp64 (default: all)")
+    ap.add_argument("--ref-sizes", default="128",
+                    help="--impl reference: comma-separated larger sample sizes whose per-zone rate is "
+                         "reported beside the 64^3 one (256 needs ~30 GB of host memory and minutes)")
+    ap.add_argument("--t-start2", type=float, default=0.15,
+                    help="second snapshot of the mixed + learned leg (0: none), where the shock front is larger")
+    ap.add_argument("--turb-steps", type=int, default=100,
+                    help="--workload turbulence: steps of each form from t = 0 (timed after --warmup)")
     return ap.parse_args()
 
 
@@ -157,47 +165,72 @@ def ref_binary():
     return b if b.exists() else None
 
 
-def run_reference_sample(steps, warmup, threads):
-    """Time the reference's own CPU path (oracle/_ref/how_ref) on the 64^3 sample;
-    returns (zone-cycles/s, kind, sample description).  Falls back to the oracle
-    port (oracle/_build/liboracle.so) when the reference build is absent."""
-    import numpy as np
-    import how_mhd as hm
-    n = REF_SAMPLE_N
-    sample = (f"blast3d_b {n}^3 (the headline problem at a size the host finishes in seconds), "
-              f"{steps} timed SSPRK step(s) after {warmup} warm-up, {threads} OpenMP threads")
-    text = workload_text(n, "fp64")
-    p = hm.read_parameters(text)
-    q = hm.problem_state(p)
+def reference_input(n):
+    """input.in of the workload at n^3 with the reference's own keys only
+    (src/parameters.cpp:46-111), so its parser has nothing to warn about."""
+    return (f"nx {n}\nny {n}\nnz {n}\nnt 1\ntend 1000.0\ngam 1.6666666666666667\ncour 0.4\n"
+            f"problem blast3d_b\nx1bc periodic\nx2bc periodic\nx3bc periodic\nrhomin 1e-6\npgmin 1e-6\n")
+
+
+def run_reference_sample(n, steps, warmup, threads, timeout=3600):
+    """Time the reference's own CPU path on blast3d_b n^3: oracle/_ref/how_ref,
+    the reference's src/*.cpp built from its sources, which makes the initial
+    state itself (the benchmark problems are registered into its registry
+    through its RegisterProblem, oracle/ref_problems.cpp) and runs `warmup`
+    untimed then `steps` timed main-loop steps.  Returns a dict (zone-cycles/s,
+    kind "reference", peak RSS of that process).  If the reference build is
+    absent or fails, its return code and stderr are logged and the oracle port
+    (oracle/_build/liboracle.so) is timed instead (kind "port")."""
     binp = ref_binary()
+    why = "reference build oracle/_ref/how_ref absent"
     if binp is not None:
-        sys.path.insert(0, str(REPO / "tests"))
-        from howtest import write_dump
         with tempfile.TemporaryDirectory() as td:
             inp = Path(td) / "in.txt"
-            inp.write_text(text)
-            st = Path(td) / "state.bin"
-            write_dump(st, {"q": q})
+            inp.write_text(reference_input(n))
+            out, err = Path(td) / "out.txt", Path(td) / "err.txt"
             env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-            r = subprocess.run([str(binp), str(inp), "/dev/null", "--state", str(st), "--steps", str(steps),
-                                "--warmup", str(warmup), "--time-only", "--threads", str(threads)],
-                               capture_output=True, text=True, env=env, timeout=3600)
-            if r.returncode == 0:
-                js = json.loads(r.stdout.strip().splitlines()[-1])
-                return js["zone_cycles_per_s"], "reference", sample
-    # oracle port
+            with open(out, "w") as fo, open(err, "w") as fe:
+                proc = subprocess.Popen([str(binp), str(inp), "/dev/null", "--steps", str(steps), "--warmup",
+                                         str(warmup), "--time-only", "--threads", str(threads)],
+                                        stdout=fo, stderr=fe, env=env)
+                t0 = time.perf_counter()
+                while True:
+                    pid, status, ru = os.wait4(proc.pid, os.WNOHANG)
+                    if pid:
+                        break
+                    if time.perf_counter() - t0 > timeout:
+                        proc.kill()
+                        pid, status, ru = os.wait4(proc.pid, 0)
+                        break
+                    time.sleep(0.05)
+            rc = os.waitstatus_to_exitcode(status)
+            if rc == 0:
+                js = json.loads(out.read_text().strip().splitlines()[-1])
+                return {"zone_cycles_per_s": js["zone_cycles_per_s"], "kind": "reference", "n": n,
+                        "steps": steps, "warmup": warmup, "threads": threads, "wall_s": js["wall_s"],
+                        "peak_rss_gb": ru.ru_maxrss / 1e6}
+            why = f"reference build exited {rc}: {err.read_text()[-400:]!r}"
+    print(f"bench: {why}; timing the oracle port instead", file=sys.stderr, flush=True)
     sys.path.insert(0, str(REPO / "tests"))
     from howtest import CPUOracle, oracle_lib
     oracle_lib().oracle_set_threads(threads)
     o = CPUOracle(n, n, n, gam=5.0 / 3.0, rhomin=1e-6, pgmin=1e-6)
-    o.set_state(q)
+    o.init_problem("blast3d_b")
     for _ in range(warmup):
         o.ssprk(o.tstep())
     t0 = time.perf_counter()
     for _ in range(steps):
         o.ssprk(o.tstep())
     el = time.perf_counter() - t0
-    return n ** 3 * steps / el, "port", sample.replace("OpenMP", "OpenMP (oracle port)")
+    return {"zone_cycles_per_s": n ** 3 * steps / el, "kind": "port", "n": n, "steps": steps, "warmup": warmup,
+            "threads": threads, "wall_s": el, "why_port": why}
+
+
+def sample_text(r):
+    who = "the reference's own sources (oracle/_ref/how_ref)" if r["kind"] == "reference" else "the oracle port"
+    return (f"blast3d_b {r['n']}^3 from t = 0 (the headline problem at a size the host finishes in seconds; the "
+            f"reference's per-zone work does not depend on the state), {r['steps']} timed SSPRK step(s) after "
+            f"{r['warmup']} warm-up, {r['threads']} OpenMP threads, {who}")
 
 
 def host_threads():
@@ -207,24 +240,45 @@ def host_threads():
         return os.cpu_count() or 1
 
 
+def headline_config(n, world):
+    """`config` of the headline workload, shared by both arms."""
+    return {"workload": f"3-D MHD blast {n}^3 (blast3d_b), periodic, gam 5/3, cour 0.4, floors 1e-6; "
+                        f"SSPRK(5,4) + characteristic WENO5/LLF + 4th-order CT; `value` = plain FP64, "
+                        f"`mixed_learned` = FP32 characteristic part + learned WENO routing",
+            "n": n, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "state 12.5 GB per replica >> 126 MB L2: every step streams from HBM, no flush"}
+
+
 # ---------------------------------------------------------------- reference arm
 def bench_reference(args):
+    """The reference's own CPU implementation of the time step, timed on the
+    host cores: each bench step is one SSPRK step of a bounded sample of the
+    headline workload (blast3d_b at REF_SAMPLE_N^3); the per-zone rate at
+    larger samples (--ref-sizes) is reported beside it."""
     world, rank, local = dist_info()
     if rank != 0:
         return 0
     threads = host_threads()
     t0 = time.perf_counter()
-    zcs, kind, sample = run_reference_sample(max(args.steps, 1), args.warmup, threads)
+    main = run_reference_sample(REF_SAMPLE_N, max(args.steps, 1), args.warmup, threads)
+    zcs = main["zone_cycles_per_s"]
+    sizes = {}
+    for m in [int(x) for x in args.ref_sizes.split(",") if x.strip()]:
+        if m == REF_SAMPLE_N:
+            continue
+        sizes[f"{m}^3"] = run_reference_sample(m, 2 if m <= 128 else 1, 1 if m <= 128 else 0, threads)
     n3 = REF_SAMPLE_N ** 3
     line = {
         "impl": "reference", "metric": METRIC, "value": zcs, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n3 / zcs,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"3-D MHD blast (blast3d_b) {REF_SAMPLE_N}^3 sample of the 256^3 workload, "
-                               "reference Kokkos/OpenMP path built from its own sources"},
-        "cpu_baseline": {"value": zcs, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "config": headline_config(args.n, world),
+        "cpu_baseline": {"value": zcs, "unit": UNIT, "cores": threads, "kind": main["kind"],
+                         "sample": sample_text(main)},
         "e2e": {"value": zcs, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "sample": main,
+        "larger_samples": sizes,
         "wall_s": time.perf_counter() - t0,
     }
     print(json.dumps(line), flush=True)
@@ -276,6 +330,15 @@ def div4_max(b, n, d):
     return float(np.abs(D(b[0], 0) + D(b[1], 1) + D(b[2], 2)).max())
 
 
+def div_report(b, n, dx):
+    """max |div4 B| and that value relative to max |B| / dx (the size of one
+    face-B difference quotient, i.e. the round-off scale of the measure)."""
+    import numpy as np
+    dv = div4_max(b, n, dx)
+    bmax = float(max(np.abs(x).max() for x in b))
+    return {"max_div_b": dv, "max_div_b_rel": dv / (bmax / dx) if bmax > 0 else None}
+
+
 def bench_ours(args):
     import ctypes
     import numpy as np
@@ -291,6 +354,7 @@ def bench_ours(args):
                                 device_id=torch.device("cuda", local))
     n = args.n
     fp64_peak = ctypes_peak(hm)
+    s_act = slice(3, n + 3)
 
     def barrier():
         if world > 1:
@@ -298,31 +362,42 @@ def bench_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # The timed steps start from the blast at t_start (evolved by the fast path,
-    # so every leg starts from the same mid-run state with a shock in the box).
+    # The timed steps start from the blast at t_start (and, for the second
+    # snapshot, t_start2), evolved by the fast path so every leg starts from
+    # the same mid-run state with a shock in the box.
     t0_prep = time.perf_counter()
-    q_start = b_start = None
-    t_start = 0.0
-    if args.t_start > 0:
-        pp = hm.read_parameters(workload_text(n, "mixed", tend=args.t_start, router="on"))
-        with hm.Domain(pp) as d:
-            d.init_problem()
-            t_start, _, _ = d.run(0.0, -1)
-            q_start = d.get_state(0)
-            b_start = d.get_face_b(0)
+    snaps = []   # (t, q, face B)
+    targets = [t for t in (args.t_start, args.t_start2 if not args.no_fast else 0.0) if t > 0]
+    if targets:
+        # each snapshot: a run with tend = that time (the main loop's clamp
+        # lands on it exactly), continued from the previous snapshot
+        t_now, q_now, b_now = 0.0, None, None
+        for tt in sorted(targets):
+            pp = hm.read_parameters(workload_text(n, "mixed", tend=tt, router="on"))
+            with hm.Domain(pp) as d:
+                if q_now is None:
+                    d.init_problem()
+                else:
+                    d.set_state(q_now)
+                    d.set_face_b(*b_now)
+                t_now, _, _ = d.run(t_now, -1)
+                q_now, b_now = d.get_state(0), d.get_face_b(0)
+            snaps.append((t_now, q_now, b_now))
+    else:
+        snaps.append((0.0, None, None))
     prep_s = time.perf_counter() - t0_prep
 
-    def make_domain(precision, router):
+    def make_domain(precision, router, snap):
         p = hm.read_parameters(workload_text(n, precision, router=router))
         dom = hm.Domain(p)
-        if q_start is not None:
-            dom.set_state(q_start)
-            dom.set_face_b(*b_start)
+        if snap[1] is not None:
+            dom.set_state(snap[1])
+            dom.set_face_b(*snap[2])
         else:
             dom.init_problem()
         return p, dom
 
-    def timed_leg(dom, clocks_too):
+    def timed_leg(dom, t_start, clocks_too):
         """warm-up, then exactly K steps between barriers, CUDA events on the
         library's stream; returns ms, launches, sweep ms, sweep launches, clocks."""
         stream = torch.cuda.ExternalStream(dom.stream)
@@ -350,92 +425,95 @@ def bench_ours(args):
         clocks = sampler.stop() if sampler else None
         return max_over_ranks(ms, world, "cuda"), launches, sweep_ms.value, sweep_n.value, clocks
 
-    # ---- plain FP64 (the reference's method)
-    p, dom = make_domain("fp64", "off")
-    ms, launches, sweep_ms, sweep_n, clocks = timed_leg(dom, True)
-    value = replica_value(world, n ** 3, args.steps, ms)
-    rho64 = None
-    if not args.no_fast and rank == 0:
-        q64 = dom.get_state(0)
-        rho64 = q64[0, 3:n + 3, 3:n + 3, 3:n + 3].copy()
-        e64 = q64[7, 3:n + 3, 3:n + 3, 3:n + 3].copy()
-        del q64
-
-    # ---- e2e through the C ABI with pinned host buffers
-    e2e = None
-    if not args.no_e2e:
-        stream = torch.cuda.ExternalStream(dom.stream)
-        shp = (8,) + tuple(p.shape)
-        qh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
-        bh = [torch.empty(tuple(p.shape), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
-        dom.get_state(0, out=qh)
-        dom.get_face_b_into(*bh)
-        barrier()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(args.steps):
-            dom.set_state(qh)
-            dom.set_face_b(*bh)
-            dt = dom.tstep()
-            dom.ssprk(dt)
+    def fp64_leg(snap, clocks_too, with_e2e):
+        p, dom = make_domain("fp64", "off", snap)
+        ms, launches, sweep_ms, sweep_n, clocks = timed_leg(dom, snap[0], clocks_too)
+        value = replica_value(world, n ** 3, args.steps, ms)
+        ref = None
+        if rank == 0:
+            q64 = dom.get_state(0)
+            b64 = dom.get_face_b(0)
+            ref = (q64[0, s_act, s_act, s_act].copy(), q64[7, s_act, s_act, s_act].copy(), div_report(b64, n, p.dx))
+            del q64, b64
+        e2e = None
+        if with_e2e:
+            stream = torch.cuda.ExternalStream(dom.stream)
+            shp = (8,) + tuple(p.shape)
+            qh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
+            bh = [torch.empty(tuple(p.shape), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
             dom.get_state(0, out=qh)
             dom.get_face_b_into(*bh)
-        f1.record(stream)
-        barrier()
-        ems = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
-        nbytes = 8 * int(np.prod(shp)) + 3 * 8 * int(np.prod(p.shape))
-        e2e = {"value": world * n ** 3 * args.steps / (ems * 1e-3), "unit": UNIT,
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "ms_per_step": ems / args.steps, "path": "plain FP64 through the C ABI (how_set_state, "
-                                                         "how_tstep, how_ssprk, how_get_state)"}
-        del qh, bh
-    dom.close()
+            barrier()
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(args.steps):
+                dom.set_state(qh)
+                dom.set_face_b(*bh)
+                dt = dom.tstep()
+                dom.ssprk(dt)
+                dom.get_state(0, out=qh)
+                dom.get_face_b_into(*bh)
+            f1.record(stream)
+            barrier()
+            ems = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
+            nbytes = 8 * int(np.prod(shp)) + 3 * 8 * int(np.prod(p.shape))
+            e2e = {"value": world * n ** 3 * args.steps / (ems * 1e-3), "unit": UNIT,
+                   "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                   "ms_per_step": ems / args.steps, "path": "plain FP64 through the C ABI (how_set_state, "
+                                                             "how_tstep, how_ssprk, how_get_state)"}
+            del qh, bh
+        dom.close()
+        return value, ms, launches, sweep_ms, sweep_n, clocks, ref, e2e
 
-    # ---- mixed precision + learned routing (the fast form), same start, same steps
-    fast = None
-    if not args.no_fast:
-        pf, domf = make_domain("mixed", "on")
+    def fast_leg(snap, ref, value64, refresh=5):
+        pf, domf = make_domain("mixed", "on", snap)
+        if refresh != 5:
+            domf.set_router_refresh(refresh)
         domf.router_stats(reset=True)
-        fms, flaunch, fsw_ms, fsw_n, _ = timed_leg(domf, False)
+        fms, flaunch, fsw_ms, fsw_n, _ = timed_leg(domf, snap[0], False)
         full, cheap = domf.router_stats()
         fvalue = replica_value(world, n ** 3, args.steps, fms)
+        out = None
         if rank == 0:
             qf = domf.get_state(0)
             bf = domf.get_face_b(0)
-            rf = qf[0, 3:n + 3, 3:n + 3, 3:n + 3]
-            ef = qf[7, 3:n + 3, 3:n + 3, 3:n + 3]
-            w, thr = hm.default_router()
-            fast = {
-                "value": fvalue, "unit": UNIT, "ms_per_step": fms / args.steps,
-                "speedup_vs_plain_fp64": fvalue / value,
+            rf = qf[0, s_act, s_act, s_act]
+            ef = qf[7, s_act, s_act, s_act]
+            out = {
+                "t_start": snap[0], "value": fvalue, "unit": UNIT, "ms_per_step": fms / args.steps,
+                "speedup_vs_plain_fp64": fvalue / value64,
                 "full_weno_fraction": full / max(full + cheap, 1),
-                "l1_rho_vs_fp64": float(np.abs(rf - rho64).sum() / np.abs(rho64).sum()),
-                "l1_energy_vs_fp64": float(np.abs(ef - e64).sum() / np.abs(e64).sum()),
-                "max_div_b": div4_max(bf, n, pf.dx),
-                "router_threshold": thr, "gpu_launches": flaunch,
-                "sweep_avg_ms": fsw_ms / max(fsw_n, 1),
-                "note": "same start state and step count as the plain FP64 leg; L1 over active cells; the network decides once per step, the guard every stage",
+                "l1_rho_vs_fp64": float(np.abs(rf - ref[0]).sum() / np.abs(ref[0]).sum()),
+                "l1_energy_vs_fp64": float(np.abs(ef - ref[1]).sum() / np.abs(ref[1]).sum()),
+                "gpu_launches": flaunch, "sweep_avg_ms": fsw_ms / max(fsw_n, 1),
             }
+            out.update(div_report(bf, n, pf.dx))
             del qf, bf
         domf.close()
-        # the same form with the network's decisions formed at every stage
-        pf, domf = make_domain("mixed", "on")
-        domf.set_router_refresh(1)
-        domf.router_stats(reset=True)
-        sms, _, _, _, _ = timed_leg(domf, False)
-        full5, cheap5 = domf.router_stats()
+        return out
+
+    # ---- snapshot 1: plain FP64 (the reference's method), e2e, the fast form
+    value, ms, launches, sweep_ms, sweep_n, clocks, ref1, e2e = fp64_leg(snaps[0], True, not args.no_e2e)
+    fast = None
+    if not args.no_fast:
+        fast = fast_leg(snaps[0], ref1, value)
+        every = fast_leg(snaps[0], ref1, value, refresh=1)
         if rank == 0:
-            qf = domf.get_state(0)
-            rf = qf[0, 3:n + 3, 3:n + 3, 3:n + 3]
-            v5 = replica_value(world, n ** 3, args.steps, sms)
-            fast["decisions_every_stage"] = {
-                "value": v5, "ms_per_step": sms / args.steps, "speedup_vs_plain_fp64": v5 / value,
-                "full_weno_fraction": full5 / max(full5 + cheap5, 1),
-                "l1_rho_vs_fp64": float(np.abs(rf - rho64).sum() / np.abs(rho64).sum()),
-            }
-            del qf
-        domf.close()
+            w, thr = hm.default_router()
+            fast["router_threshold"] = thr
+            fast["note"] = ("same start state and step count as the plain FP64 leg; L1 over active cells; the "
+                            "network decides once per step, the guard every stage")
+            fast["decisions_every_stage"] = {k: every[k] for k in ("value", "ms_per_step", "speedup_vs_plain_fp64",
+                                                                   "full_weno_fraction", "l1_rho_vs_fp64")}
+        # ---- snapshot 2: the same comparison where the shock front is larger
+        if len(snaps) > 1:
+            v2, ms2, _, sw2, swn2, _, ref2, _ = fp64_leg(snaps[1], False, False)
+            f2 = fast_leg(snaps[1], ref2, v2)
+            if rank == 0:
+                f2["plain_fp64"] = {"value": v2, "ms_per_step": ms2 / args.steps,
+                                    "sweep_avg_ms": sw2 / max(swn2, 1), **ref2[2]}
+                fast["second_snapshot"] = f2
 
     if world > 1:
         import torch.distributed as dist
@@ -461,20 +539,19 @@ def bench_ours(args):
     }
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        threads = host_threads()
-        zcs, kind, sample = run_reference_sample(1, 1, threads)
-        cpu = {"value": zcs, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample}
+        r = run_reference_sample(REF_SAMPLE_N, 3, 1, host_threads())
+        cpu = {"value": r["zone_cycles_per_s"], "unit": UNIT, "cores": r["threads"], "kind": r["kind"],
+               "sample": sample_text(r)}
+    config = headline_config(n, world)
+    config["t_start"] = snaps[0][0]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"3-D MHD blast {n}^3 (blast3d_b), periodic, gam 5/3, cour 0.4, floors 1e-6; "
-                               f"SSPRK(5,4) + characteristic WENO5/LLF + 4th-order CT; `value` = plain FP64, "
-                               f"`mixed_learned` = FP32 characteristic part + learned WENO routing",
-                   "n": n, "t_start": t_start, "prep_s": prep_s,
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "state 12.5 GB per replica >> 126 MB L2: every step streams from HBM, no flush"},
+        "config": config,
+        "prep_s": prep_s,
+        "plain_fp64_div_b": ref1[2],
         "roofline": roofline,
         "mixed_learned": fast,
         "cpu_baseline": cpu,
@@ -654,6 +731,68 @@ def bench_output(args):
     return 0
 
 
+# ------------------------------------------------------------ turbulence arm
+def bench_turbulence(args):
+    """Learned WENO routing on decaying turbulence (problem turb3d: rho 1, p 1,
+    B = (0.5, 0, 0), velocity a seeded sum of solenoidal Fourier modes with
+    1 <= |k|/2pi <= 4 at rms 0.5) on a periodic --n^3 cube (384 by default).
+    The plain FP64 method and mixed precision + learned routing each take
+    --warmup untimed and --turb-steps device-timed steps from the same seeded
+    state; reported: zone-cycles/s of both, the fraction of interfaces routed
+    to full WENO, density / energy L1 of the routed form against FP64 after
+    the same steps, max |div B| of both."""
+    import numpy as np
+    import torch
+    import how_mhd as hm
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    n = args.n
+    s = slice(3, n + 3)
+    text = (f"nx {n}\nny {n}\nnz {n}\nnt 1\ntend 1000.0\ngam 1.6666666666666667\ncour 0.4\n"
+            f"problem turb3d\nseed 12345\nx1bc periodic\nx2bc periodic\nx3bc periodic\n")
+    out, ref = {}, None
+    for name, prec, router in (("fp64", "fp64", "off"), ("mixed+learned", "mixed", "on")):
+        p = hm.read_parameters(text + f"precision {prec}\nrouter {router}\n")
+        with hm.Domain(p) as d:
+            d.init_problem()
+            stream = torch.cuda.ExternalStream(d.stream)
+            t, _, _ = d.run(0.0, args.warmup)
+            if router == "on":
+                d.router_stats(reset=True)
+            d.sync()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t, steps, _ = d.run(t, args.turb_steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            q = d.get_state(0)
+            b = d.get_face_b(0)
+            st = d.router_stats() if router == "on" else None
+        rho, en = q[0, s, s, s].copy(), q[7, s, s, s].copy()
+        del q
+        r = {"zone_cycles_per_s": n ** 3 * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
+             "t_end": t}
+        r.update(div_report(b, n, p.dx))
+        del b
+        if st:
+            r["full_weno_fraction"] = st[0] / max(st[0] + st[1], 1)
+        if ref is None:
+            ref = (rho, en)
+        else:
+            r["l1_rho_vs_fp64"] = float(np.abs(rho - ref[0]).sum() / np.abs(ref[0]).sum())
+            r["l1_energy_vs_fp64"] = float(np.abs(en - ref[1]).sum() / np.abs(ref[1]).sum())
+            r["speedup_vs_plain_fp64"] = r["zone_cycles_per_s"] / out["fp64"]["zone_cycles_per_s"]
+        out[name] = r
+    if rank == 0:
+        print(json.dumps({"workload": f"decaying turbulence turb3d {n}^3 (seed 12345), {args.warmup} warm-up + "
+                                      f"{args.turb_steps} timed steps from t = 0 per form",
+                          "unit": UNIT, "timing": "CUDA events on the library's stream",
+                          "forms": out}), flush=True)
+    return 0
+
+
 def ctypes_peak(hm):
     import ctypes
     v = ctypes.c_double()
@@ -663,6 +802,8 @@ def ctypes_peak(hm):
 
 def main():
     args = parse()
+    if args.n is None:
+        args.n = 384 if args.workload == "turbulence" else 256
     if args.impl == "reference":
         return bench_reference(args)
     if args.workload == "ensemble":
@@ -671,6 +812,8 @@ def main():
         return bench_accuracy(args)
     if args.workload == "output":
         return bench_output(args)
+    if args.workload == "turbulence":
+        return bench_turbulence(args)
     return bench_ours(args)
 
 

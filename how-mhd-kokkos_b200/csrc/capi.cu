@@ -147,11 +147,15 @@ static int sync_and_status(Ctx& c) {
     HOW_CUDA_CHECK(cudaGetLastError());
     unsigned int st = 0;
     HOW_CUDA_CHECK(cudaMemcpy(&st, &c.dsc->status, sizeof(st), cudaMemcpyDeviceToHost));
-    if (st & (HOW_STATUS_TMA_TIMEOUT | HOW_STATUS_TMA_ALIGN)) {
-        cudaMemset(&c.dsc->status, 0, sizeof(st));
-        set_error("device status 0x%x: %s", st,
-                  (st & HOW_STATUS_TMA_ALIGN) ? "misaligned tensor copy refused" : "bounded TMA wait expired");
-        return HOW_ERR_CUDA;
+    if (st & (HOW_STATUS_TMA_TIMEOUT | HOW_STATUS_TMA_ALIGN | HOW_STATUS_NONFINITE_STATE)) {
+        HOW_CUDA_CHECK(cudaMemset(&c.dsc->status, 0, sizeof(st)));
+        if (st & (HOW_STATUS_TMA_TIMEOUT | HOW_STATUS_TMA_ALIGN)) {
+            set_error("device status 0x%x: %s", st,
+                      (st & HOW_STATUS_TMA_ALIGN) ? "misaligned tensor copy refused" : "bounded TMA wait expired");
+            return HOW_ERR_CUDA;
+        }
+        set_error("non-finite value in the conserved state (stage 0, active cells)");
+        return HOW_ERR_NONFINITE;
     }
     return HOW_OK;
 }
@@ -385,8 +389,10 @@ int how_sweep(how_ctx* c, int dir, double dt) {
     if (n <= 1) { set_error("no sweep along an axis with one cell"); return HOW_ERR_ARG; }
     if ((rc = upload_dt(c, dt))) return rc;
     c->cur_stage = 1;
-    // stage 1: copy_stage(q, 1, 0) then the sweep (src/ssprk.cpp:1288, 1306-1317)
+    // stage 1: copy_stage(q, 1, 0), copy_bfield_stage(1, 0), then the sweep
+    // (src/ssprk.cpp:1288-1289, 1306-1317)
     launch_copy_fields(*c, c->q[1], c->q[0], 8);
+    launch_copy_fields(*c, c->b[1], c->b[0], 3);
     const RKCoeff k = rk_coeff(1);
     SweepArgs a;
     a.g = c->g;
@@ -400,6 +406,26 @@ int how_sweep(how_ctx* c, int dir, double dt) {
     a.dtdl = &c->dsc->dtdl[1][dir];
     launch_sweep(*c, dir, a);
     return sync_and_status(*c);
+}
+
+int how_fluxct(how_ctx* c, int iw, double k1, double k3) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (iw < 1 || iw > 5) { set_error("fluxct stage %d out of range 1..5", iw); return HOW_ERR_ARG; }
+    const Grid& g = c->g;
+    const bool any_ct = (g.nx > 1 && g.ny > 1) || (g.ny > 1 && g.nz > 1) || (g.nx > 1 && g.nz > 1);
+    if (!any_ct) return HOW_OK;   // 1-D: fluxct returns at once (src/fluxct.cpp:793)
+    // bound_bfield(iw - 1) precedes fluxct in ssprk (src/ssprk.cpp:1319)
+    double* f[3] = {c->b[iw - 1], c->b[iw - 1] + g.fs, c->b[iw - 1] + 2 * g.fs};
+    launch_bound(*c, f, 3);
+    launch_fluxct(*c, iw, k1, k3);
+    return sync_and_status(*c);
+}
+
+int how_set_wait_limit(how_ctx* c, int expire_at_once) {
+    if (!c) { set_error("null context"); return HOW_ERR_ARG; }
+    c->wait_expire = expire_at_once ? 1 : 0;
+    return HOW_OK;
 }
 
 int how_set_precision(how_ctx* c, int mode) {
@@ -426,7 +452,9 @@ int how_run(how_ctx* c, double* time, long max_steps, long* steps, double* dts, 
             rc = sync_and_status(*c);
             if (rc) { *steps += taken; return rc; }
             const double dt = c->hsc->dt;
-            if (!(dt > 0.0)) {
+            // src/main.cpp:175-183: a non-positive dt stops the run (a NaN dt
+            // passes this test there too, and the time check below stops it)
+            if (dt <= 0.0) {
                 *steps += taken;
                 set_error("non-positive dt detected: time=%.17g target=%.17g dt=%.17g", *time, target, dt);
                 return HOW_ERR_DT;

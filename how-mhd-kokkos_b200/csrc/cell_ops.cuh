@@ -74,7 +74,9 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 // tstep (src/tstep.cpp:28-83): |v_d| + c_f,d of active cell t (x fastest).
-__device__ __forceinline__ void op_tstep_cell(const Grid& g, const double* __restrict__ q, double gam,
+// Returns false when one of the cell's eight conserved values is not finite
+// (the maxima ignore such a cell, as fmax does in the reference).
+__device__ __forceinline__ bool op_tstep_cell(const Grid& g, const double* __restrict__ q, double gam,
                                               double rhomin, double pgmin, long long t, double& mx, double& my,
                                               double& mz) {
     const int i = 3 + (int)(t % g.nx);
@@ -106,6 +108,9 @@ __device__ __forceinline__ void op_tstep_cell(const Grid& g, const double* __res
     mx = fmax(mx, fabs(vx) + lfx);
     my = fmax(my, fabs(vy) + lfy);
     mz = fmax(mz, fabs(vz) + lfz);
+    const double big = 1.7976931348623157e308;
+    return fabs(DD) <= big && fabs(Mx) <= big && fabs(My) <= big && fabs(Mz) <= big && fabs(Bx) <= big &&
+           fabs(By) <= big && fabs(Bz) <= big && fabs(EE) <= big;
 }
 
 // Block reduction of the three maxima and one atomicMax per block on the bit
@@ -338,10 +343,13 @@ __device__ __forceinline__ void op_faceb_base_cell(const Grid& g, const BArgs& a
 }
 
 // fluxct_interp_b_to_q (src/fluxct.cpp:882-897) fused with prot
-// (src/prot.cpp:10-51), which the reference runs right after on the same cells.
+// (src/prot.cpp:10-51), which the reference runs right after on the same cells
+// inside ssprk; prot_too = false leaves the interpolation alone (the
+// standalone fluxct).
 __device__ __forceinline__ void op_interp_prot_cell(const Grid& g, const double* __restrict__ b,
                                                     double* __restrict__ q, int use_x, int use_y, int use_z,
-                                                    double gam, double rhomin, double pgmin, int i, int j, int k) {
+                                                    double gam, double rhomin, double pgmin, int i, int j, int k,
+                                                    bool prot_too = true) {
     const long long c = g.idx(i, j, k);
     const long long sj = g.pitch, sk = (long long)g.pitch * g.P1, fs = g.fs;
     const double* bx = b;
@@ -359,6 +367,7 @@ __device__ __forceinline__ void op_interp_prot_cell(const Grid& g, const double*
     q[4 * fs + c] = Bx;
     q[5 * fs + c] = By;
     q[6 * fs + c] = Bz;
+    if (!prot_too) return;
     rho = fmax(rho, rhomin);
     // the four quotients of prot, each correctly rounded, from two divisions
     const double irho = 1.0 / rho, igm1 = 1.0 / (gam - 1.0);

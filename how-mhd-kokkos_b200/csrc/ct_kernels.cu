@@ -50,9 +50,9 @@ __global__ void k_faceb_base(Grid g, BArgs a) {
 
 __global__ void k_interp_prot(Grid g, const double* __restrict__ b, double* __restrict__ q,
                               int use_x, int use_y, int use_z, double gam, double rhomin,
-                              double pgmin) {
+                              double pgmin, int prot_too) {
     HOW_CELL_IJK;
-    op_interp_prot_cell(g, b, q, use_x, use_y, use_z, gam, rhomin, pgmin, i, j, k);
+    op_interp_prot_cell(g, b, q, use_x, use_y, use_z, gam, rhomin, pgmin, i, j, k, prot_too != 0);
 }
 #undef HOW_CELL_IJK
 
@@ -77,9 +77,14 @@ void launch_faceb_base(Ctx& c, int iw, double c4, double c5, int stage5) {
     launch_bound(c, bf, 3);
 }
 
-// fluxct (src/fluxct.cpp:786-899) + prot for stage iw.  Requires the sweeps of
-// the stage to have filled the CT flux arrays at active faces.
-void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5) {
+// fluxct (src/fluxct.cpp:786-899) for stage iw, followed by prot when
+// prot_too (as ssprk runs it).  Requires the sweeps of the stage to have
+// filled the CT flux arrays at active faces.  The face-B base is the stage's
+// copied (or, for stage 5, combined) base formed from b0/b2/b3 in place;
+// base_from_stage reads it from face B(iw) itself instead, as the standalone
+// fluxct does after the caller's copy_bfield_stage.
+static void run_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5, bool prot_too,
+                   bool base_from_stage) {
     const Grid& g = c.g;
     const int use_x = g.nx > 1, use_y = g.ny > 1, use_z = g.nz > 1;
     const int use_Ox = use_x && use_y, use_Oy = use_y && use_z, use_Oz = use_x && use_z;
@@ -113,13 +118,22 @@ void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int s
         launch_bound(c, fl, n);
     }
     BArgs a = make_bargs(c, iw, k1, k3, c4, c5, stage5);
+    if (base_from_stage) { a.b0 = c.b[iw]; a.stage5 = 0; }
     k_update_b<<<grid, 128, 0, c.stream>>>(g, f, a, use_Ox, use_Oy, use_Oz);
     ++c.launches;
     double* bf[3] = {c.b[iw], c.b[iw] + g.fs, c.b[iw] + 2 * g.fs};
     launch_bound(c, bf, 3);
     k_interp_prot<<<grid, 128, 0, c.stream>>>(g, c.b[iw], c.q[iw], use_x, use_y, use_z, c.p.gam,
-                                              c.p.rhomin, c.p.pgmin);
+                                              c.p.rhomin, c.p.pgmin, prot_too ? 1 : 0);
     ++c.launches;
+}
+
+void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5) {
+    run_ct(c, iw, k1, k3, c4, c5, stage5, true, false);
+}
+
+void launch_fluxct(Ctx& c, int iw, double k1, double k3) {
+    run_ct(c, iw, k1, k3, 0.0, 0.0, 0, false, true);
 }
 
 }  // namespace how

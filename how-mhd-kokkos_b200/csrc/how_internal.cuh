@@ -88,7 +88,8 @@ struct DevScalars {
     double dt_raw;                     // dt before the output-time clamp
 };
 
-enum : unsigned int { HOW_STATUS_NONFINITE_DT = 1u, HOW_STATUS_TMA_TIMEOUT = 2u, HOW_STATUS_TMA_ALIGN = 4u };
+enum : unsigned int { HOW_STATUS_NONFINITE_DT = 1u, HOW_STATUS_TMA_TIMEOUT = 2u, HOW_STATUS_TMA_ALIGN = 4u,
+                      HOW_STATUS_NONFINITE_STATE = 8u };
 
 // Arguments of one directional sweep launch.
 struct SweepArgs {
@@ -129,6 +130,10 @@ struct SweepArgs {
     const int* ens_par;                // per member: stage-0 / stage-5 buffer parity
     const int* ens_active;             // per member: 1 while it is stepping
     int ens_n, ens_stride, ens_off;
+    // failure-detection tests: nonzero makes the compute threads' tile waits
+    // give up at once (the issuer's drain of copies in flight keeps its
+    // full limit), so the launch ends early with HOW_STATUS_TMA_TIMEOUT
+    int wait_expire;
 };
 
 // Packed router weights (FP32): W1[32][6], b1[32], W2[32][32], b2[32], w3[32], b3.
@@ -170,6 +175,7 @@ struct Ctx {
     float route_thr = 0.0f, guard_jump = 0.25f, guard_floor = 100.0f;
     int route_refresh = 5;                // learned routing: fresh decisions every this many stages (1..5)
     int cur_stage = 1;                    // SSPRK stage being launched (1..5)
+    int wait_expire = 0;                  // failure-detection test hook (SweepArgs::wait_expire)
     struct DumpJob* dump = nullptr;       // asynchronous dump file in flight (output.cu)
 };
 
@@ -184,6 +190,8 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a);
 // learned-router decisions of every interface of sweep `dir` (route_prepass.cu)
 void launch_route(Ctx& c, int dir, const double* q, const unsigned char* prev, unsigned char* next);
 void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5);
+// standalone fluxct(q, iw, k1, k3): face B(iw) = k1 B(iw) + k3 B(iw-1) + CT update, no prot
+void launch_fluxct(Ctx& c, int iw, double k1, double k3);
 void launch_faceb_base(Ctx& c, int iw, double c4, double c5, int stage5);
 void launch_prot(Ctx& c, int stage);
 void launch_stage5_base(Ctx& c, double c4, double c5);

@@ -10,24 +10,24 @@
 //
 // How: the reduction keeps its per-line partial maxima in a file-scope
 // __device__ array of fixed size (HOW_NOALLOC_MAX_LINES lines x 3 doubles,
-// 6 MiB per GPU).  Every GPU that loads this library holds that array until
-// the process exits.  In host code the array's name is only a host-side
-// stand-in, so the device address is looked up once per device with
-// cudaGetSymbolAddress (with that device current) and passed to the kernels.
+// 6 MiB per GPU).  In host code the array's name is only a host-side
+// stand-in, so every call looks up its device address on the current device
+// with cudaGetSymbolAddress and passes that to the kernels (a cached address
+// would go stale after a device reset).  Under CUDA's default lazy module
+// loading, this file's module -- and with it the array -- is placed on a
+// device by the first such lookup there: the first call on each device takes
+// the 6 MiB, and the array stays until the process exits.  Callers make that
+// first call during set-up, before a memory pool reserves the device, or set
+// CUDA_MODULE_LOADING=EAGER so the array is placed when the library loads.
 #include "how_internal.cuh"
-
-#include <mutex>
 
 namespace how {
 namespace {
 
 constexpr int kNoAllocMaxLines = HOW_NOALLOC_MAX_LINES;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_cfl_line_max[3 * kNoAllocMaxLines];
 
-std::mutex g_setup_mutex;
-double* g_scratch_ptr[kMaxDevices] = {};
 
 // Pass 1: one warp per (i, j) line along k (contiguous in the reference
 // layout), lanes striding k; writes the line's three maxima of |v_d| + c_f,d
@@ -109,20 +109,14 @@ __global__ void k_cfl_finish(const double* __restrict__ line_max, long long nlin
     }
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device with that device current.
+// Device address of the scratch array on the current device (the device
+// the kernels below launch on).  The first lookup on a device places the
+// module there; later ones only read its address.
 int scratch_for_current_device(double** out) {
-    int dev = 0;
-    HOW_CUDA_CHECK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) { set_error("device ordinal %d beyond %d", dev, kMaxDevices); return HOW_ERR_ARG; }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        double* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_cfl_line_max);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_cfl_line_max)");
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    double* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_cfl_line_max);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_cfl_line_max)");
+    *out = p;
     return HOW_OK;
 }
 

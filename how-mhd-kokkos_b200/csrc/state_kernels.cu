@@ -71,14 +71,20 @@ __global__ void k_init_faceb(Grid g, const double* __restrict__ q0, double* __re
     b0[2 * g.fs + c] = (-Bz[c - sk] + 9.0 * Bz[c] + 9.0 * Bz[c + sk] - Bz[c + 2 * sk]) / 16.0;
 }
 
-// tstep (src/tstep.cpp:28-83): max over active cells of |v_d| + c_f,d.
+// tstep (src/tstep.cpp:28-83): max over active cells of |v_d| + c_f,d.  A
+// non-finite conserved value anywhere sets HOW_STATUS_NONFINITE_STATE (the
+// reference's reduction skips such cells through fmax and notices only a
+// non-finite time, src/main.cpp:207-212; here the caller learns of the bad
+// state before stepping on it).
 __global__ void k_tstep(Grid g, const double* __restrict__ q, double gam, double rhomin,
                         double pgmin, DevScalars* sc) {
     double mx = 0.0, my = 0.0, mz = 0.0;
+    bool ok = true;
     const long long ncell = (long long)g.nx * g.ny * g.nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell;
          t += (long long)gridDim.x * blockDim.x)
-        op_tstep_cell(g, q, gam, rhomin, pgmin, t, mx, my, mz);
+        ok &= op_tstep_cell(g, q, gam, rhomin, pgmin, t, mx, my, mz);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(&sc->status, HOW_STATUS_NONFINITE_STATE);
     block_max3_to(mx, my, mz, sc->vmax_bits);
 }
 

@@ -327,6 +327,9 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         return t;
     };
     const int tid = threadIdx.x;
+    // the compute threads' tile waits (a failure-detection test can make them
+    // give up at once); the drain in bail() below always keeps kWaitLimit
+    const uint32_t wait_limit = a0.wait_expire ? 0u : kWaitLimit;
     // the thread that issues and tracks the tile copies: the block's last,
     // whose warp has the least P1 work, so issuing does not delay P1
     const bool issuer = tid == NT - 1;
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
 
         // ------------------------------------------------------------ P0
         {
-            const bool ok = issued_ok && mbar_wait_bounded(&bars[buf], (par_bits >> buf) & 1u, kWaitLimit);
+            const bool ok = issued_ok && mbar_wait_bounded(&bars[buf], (par_bits >> buf) & 1u, wait_limit);
             if (__syncthreads_or(!ok)) { bail(); return; }   // results void; host sees the status
         }
         par_bits ^= 1u << buf;
@@ -1015,7 +1018,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
 
         // ------------------------------------------------------------ P5
         {
-            const bool ok = mbar_wait_bounded(&bars[2], (par_bits >> 2) & 1u, kWaitLimit);
+            const bool ok = mbar_wait_bounded(&bars[2], (par_bits >> 2) & 1u, wait_limit);
             if (__syncthreads_or(!ok)) { bail(); return; }
         }
         par_bits ^= 4u;

@@ -102,6 +102,7 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     a.guard_jump = c.guard_jump;
     a.guard_floor = c.guard_floor;
     a.ct4 = c.p.ct_avg == 4;
+    a.wait_expire = c.wait_expire;
     const bool mixed = c.precision == HOW_PREC_MIXED;
     const int mode = c.route_mode;
     if (mode == 1) {

@@ -97,6 +97,8 @@ def _load():
         "how_ssprk": ([V, ctypes.c_double], ctypes.c_int),
         "how_prot": ([V, ctypes.c_int], ctypes.c_int),
         "how_sweep": ([V, ctypes.c_int, ctypes.c_double], ctypes.c_int),
+        "how_fluxct": ([V, ctypes.c_int, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+        "how_set_wait_limit": ([V, ctypes.c_int], ctypes.c_int),
         "how_get_ct_array": ([V, ctypes.c_int, D], ctypes.c_int),
         "how_run": ([V, D, ctypes.c_long, ctypes.POINTER(ctypes.c_long), D, ctypes.c_long], ctypes.c_int),
         "how_output": ([V, ctypes.c_int, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
@@ -336,6 +338,15 @@ class Domain:
     def sweep(self, direction: int, dt: float):
         _check(_lib.how_sweep(self._h, direction, dt))
 
+    def fluxct(self, iw: int, k1: float, k3: float):
+        """fluxct(q, iw, k1, k3, par, ct) (src/fluxct.cpp:786-899) on the CT
+        flux arrays the last sweeps filled, after bound_bfield(iw - 1)."""
+        _check(_lib.how_fluxct(self._h, iw, k1, k3))
+
+    def set_wait_limit(self, expire_at_once: bool):
+        """Failure-detection tests: make the sweep kernels' tile waits give up at once."""
+        _check(_lib.how_set_wait_limit(self._h, 1 if expire_at_once else 0))
+
     def run(self, time=0.0, max_steps=-1, dts_cap=0):
         t = ctypes.c_double(time)
         s = ctypes.c_long(0)
@@ -566,3 +577,7 @@ def ssprk(dom: Domain, dt: float):
 
 def prot(dom: Domain, stage: int):
     dom.prot(stage)
+
+
+def fluxct(dom: Domain, iw: int, k1: float, k3: float):
+    dom.fluxct(iw, k1, k3)

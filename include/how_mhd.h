@@ -136,8 +136,18 @@ int how_ssprk(how_ctx* ctx, double dt);
 int how_prot(how_ctx* ctx, int stage);
 /* One directional sweep of stage 1 (src/ssprk.cpp:1000-1025, 1218-1272)
  * exactly as the reference's x_sweep/y_sweep/z_sweep would run it inside
- * stage 1 of ssprk with this dt: copies q(0) to q(1) first.  dir 0,1,2. */
+ * stage 1 of ssprk with this dt: copies q(0) to q(1) and face B(0) to face
+ * B(1) first (copy_stage, copy_bfield_stage, src/ssprk.cpp:1288-1289).
+ * dir 0,1,2.  Each call fills the two CT flux arrays of its direction. */
 int how_sweep(how_ctx* ctx, int dir, double dt);
+/* fluxct(q, iw, k1, k3, par, ct) (src/fluxct.hpp:41-42, body
+ * src/fluxct.cpp:786-899), preceded by bound_bfield(iw - 1) as ssprk runs it
+ * (src/ssprk.cpp:1319-1320): corner EMFs from the CT flux arrays the last
+ * sweeps filled, their smoothing, face B(iw) = k1 B(iw) + k3 B(iw-1) + the CT
+ * update with the dt of the last sweeps, the ghost fill of face B(iw), and
+ * the face-to-centre B into q(iw, 4..6).  No prot.  In 1-D it does nothing,
+ * as the reference returns early (src/fluxct.cpp:793).  iw 1..5. */
+int how_fluxct(how_ctx* ctx, int iw, double k1, double k3);
 /* Download a CT flux array (0..5 = fsy fsz gsx gsz hsx hsy) in the reference
  * layout, for inspection after how_sweep / how_ssprk.  Faces the sweeps
  * compute are valid; ghost entries are not filled (the EMF kernel reads
@@ -147,7 +157,12 @@ int how_get_ct_array(how_ctx* ctx, int which, double* host);
 /* Main loop (src/main.cpp:158-223) without output: advances from *time for
  * up to max_steps steps (max_steps < 0: no limit) towards tend, with the
  * reference's nt output intervals and dt clamp to each interval's end.
- * Updates *time and *steps.  dts (may be NULL) receives each step's dt. */
+ * Updates *time and *steps.  dts (may be NULL) receives each step's dt.
+ * Stops with HOW_ERR_DT on a non-positive dt (src/main.cpp:175-183) and with
+ * HOW_ERR_NONFINITE when the time becomes non-finite (src/main.cpp:207-212)
+ * or, before a step, when stage 0 holds a non-finite value (the CFL pass
+ * checks every active cell; the reference's own reduction skips such cells).
+ * how_tstep reports a non-finite state the same way. */
 int how_run(how_ctx* ctx, double* time, long max_steps, long* steps, double* dts, long dts_cap);
 
 /* Dump file of q(0), output() (src/output.cpp:555-572), in the context's
@@ -194,6 +209,13 @@ void* how_stream(how_ctx* ctx);
 int how_set_kernel_timing(how_ctx* ctx, int on);
 /* Summed device milliseconds and count of the timed sweep launches. */
 int how_get_kernel_timing(how_ctx* ctx, double* total_ms, long* launches);
+/* Failure-detection tests only (no reference counterpart): nonzero makes the
+ * sweep kernels' compute threads give up their bounded tile waits at once,
+ * so the next sweep ends early and the call returns HOW_ERR_CUDA with
+ * "bounded TMA wait expired"; the thread that issued the tile copies still
+ * waits, with its full limit, for every copy it has in flight before the
+ * block exits.  0 restores the normal waits; the context stays usable. */
+int how_set_wait_limit(how_ctx* ctx, int expire_at_once);
 /* Mean cycles per thread block of each phase of one stage-1 sweep (the
  * how_sweep semantics) -- instrumentation, no reference counterpart.
  * out[0..10] = phases (load, primitives, cell differences, routing features,
@@ -238,7 +260,8 @@ long how_ensemble_graph_launches(const how_ensemble* e);
  * each interface of each sweep to the full characteristic WENO5 or to a
  * component-wise linear-weight fifth-order flux; a hard jump/positivity guard
  * forces full WENO.  Inference runs on the tensor cores (BF16, FP32
- * accumulate) inside the sweep kernel. */
+ * accumulate) in a routing pass before the sweeps, whose decisions the sweep
+ * kernels read; the guard is evaluated inside the sweep kernels. */
 int how_router_param_count(void);
 /* the built-in trained weights and logit threshold (what `router on` uses) */
 int how_router_default(float* w, int n, float* threshold);
@@ -282,11 +305,16 @@ int how_router_infer(const float* w, const float* feats, long n, float* out_fp32
  *           tstep does (src/tstep.cpp:11-136)
  *   stream: cudaStream_t to order the work on (NULL = legacy stream)
  * The reduction keeps its partial results in one fixed device array of
- * HOW_NOALLOC_MAX_LINES x 3 doubles (6 MiB) that every GPU loading this
- * library holds until exit; nx * ny above HOW_NOALLOC_MAX_LINES is refused
- * with HOW_ERR_ARG.  The first call on each device looks up that array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
+ * HOW_NOALLOC_MAX_LINES x 3 doubles (6 MiB); nx * ny above
+ * HOW_NOALLOC_MAX_LINES is refused with HOW_ERR_ARG.  Every call looks up
+ * that array's device address (cudaGetSymbolAddress) on the current device.
+ * Under CUDA's default lazy module loading the array is placed on a device
+ * when that lookup first runs there, so the first call on each device is
+ * where those 6 MiB are taken: make it during set-up, before any stream
+ * capture and before a host memory pool reserves the device (or run with
+ * CUDA_MODULE_LOADING=EAGER, which places it when the library loads).  The
+ * array then stays until the process exits, and later calls take no device
+ * memory.  All calls share the array: calls that overlap on the GPU (other
  * streams, other threads) race and must be serialised by the caller.  The
  * call is asynchronous; read dt_dev after synchronising `stream`. */
 int how_tstep_noalloc(const double* q_dev, const how_params* p, double* dt_dev, void* stream);

@@ -805,6 +805,14 @@ int init_problem(Oracle& o, const std::string& name) {
                     const double rx = x - xc, ry = y - yc, rz = z - zc;
                     const double rr = std::sqrt(rx*rx + ry*ry + rz*rz);
                     fill_cell(o, i, j, k, 1.0, 0.0, 0.0, 0.0, 0.1, 0.0, 0.0, (rr <= r0) ? 100.0 : 1.0);
+                } else if (name == "blast3d_b") {        // the benchmark blast (the product's
+                    // problem of that name, default parameters): p 10 / 0.1 across r = 0.1,
+                    // B = (1, 1, 0) / sqrt 2
+                    const double xc = 0.5 * o.p.xsize, yc = 0.5 * o.p.ysize, zc = 0.5 * o.p.zsize;
+                    const double rx = x - xc, ry = y - yc, rz = z - zc;
+                    const double r = std::sqrt(rx*rx + ry*ry + rz*rz);
+                    const double b = 1.0 / std::sqrt(2.0);
+                    fill_cell(o, i, j, k, 1.0, 0.0, 0.0, 0.0, b, b, 0.0, (r < 0.1) ? 10.0 : 0.1);
                 } else if (name == "brio_wu") {          // src/problems/brio_wu.cpp:201-254
                     if (x < 0.5 * o.p.xsize) fill_cell(o, i, j, k, 1.0, 0, 0, 0, 0.75, 1.0, 0.0, 1.0);
                     else fill_cell(o, i, j, k, 0.125, 0, 0, 0, 0.75, -1.0, 0.0, 0.1);
@@ -924,6 +932,38 @@ void oracle_sweep(void* h, int dir, double dt, double* q1_out, double* ct_a, dou
     if (q1_out) std::memcpy(q1_out, o.qs(1, 0), 8 * o.PV * sizeof(double));
     if (ct_a) std::memcpy(ct_a, o.ct[ia].data(), o.PV * sizeof(double));
     if (ct_b) std::memcpy(ct_b, o.ct[ib].data(), o.PV * sizeof(double));
+}
+
+// stage iw = 1 up to its constrained transport (src/ssprk.cpp:1281-1317):
+// zero the CT arrays, copy q(0) and face B(0) into stage 1, bound q(0), then
+// the x, y and z sweeps with dt (the axes with n > 1).
+void oracle_stage1_sweeps(void* h, double dt) {
+    auto& o = *static_cast<Oracle*>(h);
+    for (auto& a : o.ct) std::fill(a.begin(), a.end(), 0.0);
+    const RK c = rk_coeff(1);
+    copy_stage(o, 1, 0);
+    copy_b(o, 1, 0);
+    bound_q(o, 0);
+    o.dt = dt;
+    o.dtdx = c.k2 * o.dt / o.dx;
+    o.dtdy = c.k2 * o.dt / o.dy;
+    o.dtdz = c.k2 * o.dt / o.dz;
+    if (o.nx > 1) sweep(o, 0, 1, c, o.dtdx, o.ct[0].data(), o.ct[1].data());
+    if (o.ny > 1) sweep(o, 1, 1, c, o.dtdy, o.ct[3].data(), o.ct[2].data());
+    if (o.nz > 1) sweep(o, 2, 1, c, o.dtdz, o.ct[4].data(), o.ct[5].data());
+}
+// bound_bfield(iw - 1) then fluxct(q, iw, k1, k3) (src/ssprk.cpp:1319-1320,
+// src/fluxct.cpp:786-899) on the CT arrays the last sweeps filled, with the
+// dtdx/dtdy/dtdz those sweeps used.
+void oracle_fluxct(void* h, int iw, double k1, double k3) {
+    auto& o = *static_cast<Oracle*>(h);
+    bound_b(o, iw - 1);
+    fluxct(o, iw, k1, k3);
+}
+void oracle_prot(void* h, int stage) { prot(*static_cast<Oracle*>(h), stage); }
+void oracle_get_ct(void* h, int which, double* out) {
+    auto& o = *static_cast<Oracle*>(h);
+    std::memcpy(out, o.ct[which].data(), o.PV * sizeof(double));
 }
 
 // counts: [0] primit, [1] centre, [2] interface L/R, [3] one WENO field incl.

@@ -40,6 +40,15 @@ int    oracle_run(void* h, double tend, int nt, long max_steps,
 /* stage iw = 1 only: copy, bound, ONE directional sweep (dir 0,1,2) with dt;
  * ct_a/ct_b receive the two CT flux arrays that sweep fills. */
 void   oracle_sweep(void* h, int dir, double dt, double* q1_out, double* ct_a, double* ct_b);
+/* stage iw = 1 up to its CT: zero the CT arrays, copy q(0) and face B(0)
+ * into stage 1, bound q(0), the x/y/z sweeps with dt. */
+void   oracle_stage1_sweeps(void* h, double dt);
+/* bound_bfield(iw - 1) + fluxct(q, iw, k1, k3) on the CT arrays the last
+ * sweeps filled; prot(q, stage); a CT array (0..11 = fsy fsz gsx gsz hsx hsy
+ * Ox2 Oy2 Oz2 Ox Oy Oz). */
+void   oracle_fluxct(void* h, int iw, double k1, double k3);
+void   oracle_prot(void* h, int stage);
+void   oracle_get_ct(void* h, int which, double* out);
 void   oracle_set_threads(int n);
 void   oracle_set_ct_avg(int points);   /* 2 (reference) or 4 */
 /* algorithmic FP64 operation counts (add/sub/mul/div/sqrt/max/abs as 1) of the

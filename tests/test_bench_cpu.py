@@ -52,10 +52,18 @@ def test_replica_timing_is_max_over_ranks_gloo():
 
 @pytest.mark.skipif(not REF_BIN.exists(), reason="reference build absent")
 def test_reference_arm_prints_contract_line():
-    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=REPO)
+    """The reference arm runs the reference's own build on the headline
+    problem without this library: pointed at a library path that does not
+    exist, it must still succeed.  Its `config` is our arm's."""
+    env = dict(os.environ, HOW_MHD_LIB="/nonexistent/libhowmhd.so")
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--steps", "2",
+                        "--warmup", "0", "--ref-sizes", ""], capture_output=True, text=True, timeout=600, cwd=REPO,
+                       env=env)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["unit"] == "zone-cycles/s"
     assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["value"] > 0
+    assert line["steps"] == 2 and line["sample"]["steps"] == 2
+    import bench
+    assert line["config"] == bench.headline_config(256, 1)

@@ -3,20 +3,29 @@
 Bar (FP64 path): relative L1 per conserved variable <= 1e-12 after 10 steps,
 dt identical to 1e-14 relative, face B to 1e-12.  Comparisons use active cells
 only: the reference leaves collapsed-axis ghost planes stale (2-D/1-D) and its
-ghost cells are refilled every stage."""
+ghost cells are refilled every stage.  Every comparison reports the figures it
+achieved through the `parity_record` fixture."""
+import os
+
 import numpy as np
 import pytest
 
-from howtest import CPUOracle, active, rel_l1
+from howtest import CPUOracle, active, oracle_lib, rel_l1
 
 pytestmark = pytest.mark.gpu
 
 TOL_Q = 1e-12
-# dt of the fast FP64 path: the reference's own dt moves by up to 4.7e-14
-# (Orszag-Tang, 10 steps) when its initial state is perturbed by 1e-16, so a
-# path that rounds differently cannot be held to 1e-14; 1e-13 is ~2x that
-# self-sensitivity.  The bit-reproducing mode is held to 0.
-TOL_DT = 1e-13
+# dt bar of the north star: 1e-14 relative, per step.
+TOL_DT = 1e-14
+# Cases held to a looser dt bar, with the reason: the reference's own dt moves
+# by 4.7e-14 (Orszag-Tang, 10 steps) when its initial state is perturbed by
+# 1e-16, so a path that rounds differently can miss 1e-14 there.
+TOL_DT_CASE = {}
+
+
+def _dt_err(dts, odts):
+    dts, odts = np.asarray(dts, dtype=np.float64), np.asarray(odts, dtype=np.float64)
+    return float(np.max(np.abs(dts - odts) / np.abs(odts))) if len(odts) else 0.0
 
 
 def _hm():
@@ -83,22 +92,24 @@ def _run_both(prob, n, bc, gam, steps, q_override=None):
 
 
 @pytest.mark.parametrize("name,prob,n,bc,gam,steps", CASES, ids=[c[0] for c in CASES])
-def test_run_parity(name, prob, n, bc, gam, steps):
+def test_run_parity(name, prob, n, bc, gam, steps, parity_record):
     hm, p, dom, o, dts, odts = _run_both(prob, n, bc, gam, steps)
-    np.testing.assert_allclose(dts, odts, rtol=TOL_DT, atol=0)
     qg = active(dom.get_state(0), *n)
     qo = active(o.get_q(0), *n)
     err = rel_l1(qg, qo)
-    assert np.all(err <= TOL_Q), f"{name}: rel L1 per var {err}"
     bg = dom.get_face_b(0)
     bo = o.get_faceb(0)
+    eb = [rel_l1(active(bg[c], *n)[None], active(bo[c], *n)[None])[0] for c in range(3)]
+    dte = _dt_err(dts, odts)
+    parity_record(case=name, steps=steps, max_rel_dt=dte, rel_l1_q=err, rel_l1_faceb=eb)
+    assert dte <= TOL_DT_CASE.get(name, TOL_DT), f"{name}: max relative dt error {dte:.3e}"
+    assert np.all(err <= TOL_Q), f"{name}: rel L1 per var {err}"
     for c in range(3):
-        e = rel_l1(active(bg[c], *n)[None], active(bo[c], *n)[None])[0]
-        assert e <= TOL_Q, f"{name}: face B{c} rel L1 {e}"
+        assert eb[c] <= TOL_Q, f"{name}: face B{c} rel L1 {eb[c]}"
 
 
 @pytest.mark.parametrize("name,prob,n,bc,gam,steps", ILL, ids=[c[0] for c in ILL])
-def test_run_parity_ill_conditioned(name, prob, n, bc, gam, steps):
+def test_run_parity_ill_conditioned(name, prob, n, bc, gam, steps, parity_record):
     hm, p, dom, o, dts, odts = _run_both(prob, n, bc, gam, steps)
     qg = active(dom.get_state(0), *n)
     qo = active(o.get_q(0), *n)
@@ -113,6 +124,7 @@ def test_run_parity_ill_conditioned(name, prob, n, bc, gam, steps):
     o2.run(10.0, 1, steps)
     sens = rel_l1(active(o2.get_q(0), *n), qo)
     bound = 10.0 * np.maximum(sens, 1e-13)
+    parity_record(case=name, steps=steps, max_rel_dt=_dt_err(dts, odts), rel_l1_q=err, oracle_self_sensitivity=sens)
     assert np.all(err <= bound), f"{name}: rel L1 {err} vs 10x self-sensitivity {bound}"
 
 
@@ -137,7 +149,7 @@ def test_bound_collapsed_axis_bitwise():
     np.testing.assert_array_equal(dom.get_state(0), o.get_q(0))
 
 
-def test_init_faceb_and_tstep():
+def test_init_faceb_and_tstep(parity_record):
     hm, p, dom, o = _setup("mpi_smooth3d", (24, 20, 16), ("periodic",) * 3, 5.0 / 3.0)
     q = _perturbed_state(hm, p, 3)
     dom.set_state(q)
@@ -146,11 +158,13 @@ def test_init_faceb_and_tstep():
     o.set_state(q)
     for c, (bg, bo) in enumerate(zip(dom.get_face_b(0), o.get_faceb(0))):
         np.testing.assert_allclose(active(bg, 24, 20, 16), active(bo, 24, 20, 16), rtol=1e-14, atol=1e-15)
-    assert abs(dom.tstep() / o.tstep() - 1.0) <= TOL_DT
+    dte = abs(dom.tstep() / o.tstep() - 1.0)
+    parity_record(case="tstep_smooth_perturbed", max_rel_dt=dte)
+    assert dte <= TOL_DT
 
 
 @pytest.mark.parametrize("direction", [0, 1, 2])
-def test_single_sweep(direction):
+def test_single_sweep(direction, parity_record):
     n = (36, 20, 18)
     hm, p, dom, o = _setup("mpi_smooth3d", n, ("periodic", "open", "periodic"), 5.0 / 3.0)
     q = _perturbed_state(hm, p, 10 + direction, amp=0.05)
@@ -163,6 +177,7 @@ def test_single_sweep(direction):
     dom.sweep(direction, dt)
     q1g = dom.get_state(1)
     err = rel_l1(active(q1g, *n), active(q1o, *n))
+    parity_record(case=f"sweep{direction}", rel_l1_q1=err)
     assert np.all(err <= TOL_Q), f"sweep {direction}: {err}"
     ia, ib = [(0, 1), (3, 2), (4, 5)][direction]
     # CT faces: padded face index 2..n+2 along the sweep, active transverse
@@ -199,3 +214,152 @@ def test_ct_avg4_vs_oracle():
         sc = np.abs(b[v]).sum()
         if sc > 0:
             assert np.abs(a[v] - b[v]).sum() <= 1e-12 * sc, v
+
+
+# ------------------------------------------------ standalone path functions
+@pytest.mark.parametrize("n,bc", [((20, 14, 12), ("periodic", "open", "periodic")),
+                                  ((24, 18, 1), ("open", "periodic", "periodic")),
+                                  ((16, 1, 12), ("periodic", "periodic", "open"))],
+                         ids=["3d_mixed", "2d_xy_open", "2d_xz_open"])
+@pytest.mark.parametrize("iw,k1,k3", [(1, 1.0, 0.0), (1, 0.44437049406734, 0.55562950593266)],
+                         ids=["stage1", "combined"])
+def test_fluxct_vs_oracle(n, bc, iw, k1, k3, parity_record):
+    """how_fluxct after the three single sweeps of stage 1 against the
+    oracle's fluxct (src/fluxct.cpp:786-899) on the same CT flux arrays: face
+    B(1) and the face-to-centre B in q(1, 4..6), relative L1 <= 1e-12."""
+    hm, p, dom, o = _setup("mpi_smooth3d", n, bc, 5.0 / 3.0)
+    q = _perturbed_state(hm, p, 40 + n[2], amp=0.05)
+    dom.set_state(q)
+    dom.bound(0)
+    dom.initialize_bfield_from_q()
+    o.set_state(q)
+    dt = 0.8 * o.tstep()
+    o.stage1_sweeps(dt)
+    o.fluxct(iw, k1, k3)
+    for d in range(3):
+        if n[d] > 1:
+            dom.sweep(d, dt)
+    dom.fluxct(iw, k1, k3)
+    bg, bo = dom.get_face_b(1), o.get_faceb(1)
+    eb = [rel_l1(active(bg[c], *n)[None], active(bo[c], *n)[None])[0] for c in range(3)]
+    qg, qo = active(dom.get_state(1), *n), active(o.get_q(1), *n)
+    eq = [rel_l1(qg[v][None], qo[v][None])[0] for v in (4, 5, 6)]
+    parity_record(case=f"fluxct_{n}_{bc}_k1={k1}", rel_l1_faceb=eb, rel_l1_cell_b=eq)
+    assert max(eb) <= TOL_Q, eb
+    assert max(eq) <= TOL_Q, eq
+
+
+def test_fluxct_1d_is_a_no_op():
+    """In 1-D the reference's fluxct returns at once (src/fluxct.cpp:793)."""
+    hm, p, dom, o = _setup("brio_wu", (64, 1, 1), ("open",) * 3, 2.0)
+    dom.init_problem()
+    b0 = dom.get_face_b(1)
+    q1 = dom.get_state(1)
+    dom.fluxct(1, 1.0, 0.0)
+    for a, b in zip(dom.get_face_b(1), b0):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(dom.get_state(1), q1)
+
+
+def test_prot_vs_oracle(parity_record):
+    """how_prot (src/prot.cpp:10-51) on a state with cells below both floors."""
+    n = (18, 12, 10)
+    hm, p, dom, o = _setup("mpi_smooth3d", n, ("periodic",) * 3, 5.0 / 3.0, rhomin=1e-3, pgmin=1e-3)
+    q = _perturbed_state(hm, p, 7, amp=0.05)
+    a = active(q, *n)
+    rng = np.random.default_rng(8)
+    low = rng.random(a.shape[1:]) < 0.1
+    a[0][low] = 1e-5                                  # density below rhomin
+    hot = rng.random(a.shape[1:]) < 0.1
+    kin_mag = 0.5 * ((a[1:4] ** 2).sum(0) / np.maximum(a[0], 1e-3) + (a[4:7] ** 2).sum(0))
+    a[7][hot] = kin_mag[hot]                          # pressure ~0, below pgmin
+    dom.set_state(q, stage=2)
+    o.set_q(2, q)
+    dom.prot(2)
+    o.prot(2)
+    qg, qo = active(dom.get_state(2), *n), active(o.get_q(2), *n)
+    np.testing.assert_array_equal(qg[:7], qo[:7])     # rho floored exactly; m, B untouched
+    rel = float(np.max(np.abs(qg[7] - qo[7]) / np.abs(qo[7])))
+    parity_record(case="prot", max_rel_E=rel, floored_rho=int(low.sum()), floored_p=int(hot.sum()))
+    assert rel <= 1e-14, rel
+
+
+@pytest.mark.parametrize("n,bc", [((10, 7, 5), ("periodic", "open", "periodic")),
+                                  ((6, 1, 2), ("open", "periodic", "open"))])
+def test_bound_bfield_vs_oracle(n, bc):
+    """how_bound_bfield (src/fluxct.cpp:481-490), bit for bit, including the
+    n = 1 and n = 2 axes' in-place fill order."""
+    hm, p, dom, o = _setup("uniform", n, bc, 5.0 / 3.0)
+    rng = np.random.default_rng(9)
+    b = [rng.standard_normal(p.shape) for _ in range(3)]
+    dom.set_face_b(*b, stage=3)
+    dom.bound_bfield(3)
+    o.set_faceb_stage(3, b)
+    o.bound_bfield(3)
+    for a, r in zip(dom.get_face_b(3), o.get_faceb(3)):
+        np.testing.assert_array_equal(a, r)
+
+
+# ---------------------------------------------------- configurations at size
+def test_orszag_tang_128_to_tend(parity_record):
+    """Config 0 through the main loop to tend = 0.5 (src/main.cpp:158-234):
+    the whole dt sequence, the state and face B at tend against the oracle.
+    765 steps.  The oracle itself moves by 1.3e-13 - 4.3e-13 (relative L1)
+    at tend under a 1e-16 perturbation of its initial state; the bar is 1e-11.
+    The last step is clamped to tend (dt = tend - time), where a 1e-16 change
+    of the time is a large relative change of dt: it is compared in absolute
+    terms against the run's typical dt."""
+    n = (128, 128, 1)
+    hm, p, dom, o = _setup("orszag_tang", n, ("periodic",) * 3, 5.0 / 3.0, tend=0.5)
+    oracle_lib().oracle_set_threads(os.cpu_count() or 1)
+    with dom:
+        dom.init_problem()
+        t, s, dts = dom.run(0.0, -1, dts_cap=10000)
+        qg = active(dom.get_state(0), *n)
+        bg = dom.get_face_b(0)
+    o.set_state(hm.problem_state(p))
+    rc, to, odts = o.run(0.5, 1)
+    assert rc == 0 and s == len(odts), (s, len(odts))
+    assert t == 0.5 and to == 0.5
+    dte = _dt_err(dts[:-1], odts[:-1])
+    last = abs(dts[-1] - odts[-1]) / float(np.median(odts))
+    err = rel_l1(qg, active(o.get_q(0), *n))
+    bo = o.get_faceb(0)
+    eb = [rel_l1(active(bg[c], *n)[None], active(bo[c], *n)[None])[0] for c in range(2)]
+    parity_record(case="ot128_tend0.5", steps=s, max_rel_dt_but_last=dte, last_dt_err_vs_median=last,
+                  rel_l1_q=err, rel_l1_faceb=eb)
+    assert dte <= 1e-11 and last <= 1e-11, (dte, last)
+    assert np.all(err <= 1e-11), err
+    assert max(eb) <= 1e-11, eb
+
+
+def test_blast3d_b_headline_size_fp64_10_steps(parity_record):
+    """The headline workload (blast3d_b 256^3, plain FP64) for 10 steps from
+    t = 0 against the oracle port: relative L1 <= 1e-12 per variable, face B,
+    dt.  The oracle needs ~16 GB of host memory at 256^3; with less the test
+    runs 128^3 and records the size it ran."""
+    import psutil
+    n1 = 256 if psutil.virtual_memory().available > 32e9 else 128
+    n = (n1, n1, n1)
+    hm, p, dom, o = _setup("blast3d_b", n, ("periodic",) * 3, 5.0 / 3.0, rhomin=1e-6, pgmin=1e-6)
+    oracle_lib().oracle_set_threads(os.cpu_count() or 1)
+    steps = 10
+    with dom:
+        dom.init_problem()
+        t, s, dts = dom.run(0.0, steps, dts_cap=steps)
+        qg = active(dom.get_state(0), *n)
+        bg = [active(b, *n).copy() for b in dom.get_face_b(0)]
+    q0 = hm.problem_state(p)
+    o.set_state(q0)
+    del q0
+    rc, to, odts = o.run(10.0, 1, steps)
+    assert s == steps and len(odts) == steps
+    err = rel_l1(qg, active(o.get_q(0), *n))
+    del qg
+    bo = o.get_faceb(0)
+    eb = [rel_l1(bg[c][None], active(bo[c], *n)[None])[0] for c in range(3)]
+    dte = _dt_err(dts, odts)
+    parity_record(case=f"blast3d_b_{n1}^3_fp64", steps=steps, max_rel_dt=dte, rel_l1_q=err, rel_l1_faceb=eb)
+    assert dte <= TOL_DT_CASE.get("blast3d_b_headline", TOL_DT), dte
+    assert np.all(err <= TOL_Q), err
+    assert max(eb) <= TOL_Q, eb

@@ -86,7 +86,8 @@ def test_register_problem_from_python():
 @pytest.mark.parametrize("prob,n,gam", [
     ("orszag_tang", (24, 20, 1), 5.0 / 3.0), ("blast3d", (12, 10, 8), 5.0 / 3.0),
     ("brio_wu", (50, 1, 1), 2.0), ("mhd_rotor", (20, 24, 1), 1.4),
-    ("uniform", (6, 5, 4), 5.0 / 3.0), ("mpi_smooth3d", (10, 8, 6), 5.0 / 3.0)])
+    ("uniform", (6, 5, 4), 5.0 / 3.0), ("mpi_smooth3d", (10, 8, 6), 5.0 / 3.0),
+    ("blast3d_b", (14, 12, 10), 5.0 / 3.0)])
 def test_initial_conditions_bit_equal_to_restatement(prob, n, gam):
     p = hm.make_parameters(nx=n[0], ny=n[1], nz=n[2], nt=1, tend=1.0, gam=gam, problem=prob)
     q = hm.problem_state(p)

@@ -132,3 +132,19 @@ def test_oracle_ct_average_order_on_alfven():
     o4 = np.log2(err(8, 4) / err(16, 4))
     assert o2 < 2.2, o2
     assert o4 > 4.0, o4
+
+
+@needs_ref
+@pytest.mark.parametrize("prob,n", [("blast3d_b", (20, 18, 16)), ("alfven3d", (12, 10, 8)),
+                                    ("turb3d", (16, 12, 10)), ("alfven3d", (24, 1, 1))])
+def test_reference_build_problems_bit_equal_to_product(tmp_path, prob, n):
+    """The benchmark problems the reference lacks are registered into the
+    reference build through its own RegisterProblem (oracle/ref_problems.cpp);
+    with default parameters their states equal the product's bit for bit, so
+    the reference arm of the benchmark builds its state without the product."""
+    hm = pytest.importorskip("how_mhd")
+    inp = write_input(tmp_path / "in.txt", nx=n[0], ny=n[1], nz=n[2], nt=1, tend=1.0, problem=prob,
+                      x1bc="periodic", x2bc="periodic", x3bc="periodic")
+    d = run_ref(inp, tmp_path / "out.bin", "--steps", 0)
+    p = hm.make_parameters(nx=n[0], ny=n[1], nz=n[2], nt=1, tend=1.0, problem=prob)
+    np.testing.assert_array_equal(active(d["q"], *n), active(hm.problem_state(p), *n))

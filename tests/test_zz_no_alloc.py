@@ -42,12 +42,18 @@ def test_noalloc_tstep_matches_context_tstep(n, problem):
     q_dev = torch.from_numpy(q).cuda()
     dt_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    for _ in range(2):
+    for call in range(2):
         dt_dev.zero_()
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         rc = lib.how_tstep_noalloc(ctypes.c_void_p(q_dev.data_ptr()), ctypes.byref(p),
                                    ctypes.c_void_p(dt_dev.data_ptr()), ctypes.c_void_p(stream))
         assert rc == 0, lib.how_last_error().decode()
         torch.cuda.synchronize()
+        if call == 1:
+            # after the first call on this device (which may place the module
+            # and its fixed array), a call takes no device memory
+            assert torch.cuda.mem_get_info()[0] == free_before
         dt = float(dt_dev.item())
         assert abs(dt / dt_ctx - 1.0) <= TOL_DT, (dt, dt_ctx)
 
