@@ -71,7 +71,7 @@ int encode_tensor_map_4d(CUtensorMap* map, const void* base, const uint64_t dims
 // are folded away: the first sweep reads the RK base directly, every CT
 // flux the EMFs read is rewritten by the sweeps before its ghost fill, and
 // q(iw-1) already had its ghosts filled at the end of the previous stage.
-static void run_stage(Ctx& c, int iw) {
+void stage_sweeps(Ctx& c, int iw) {
     const Grid& g = c.g;
     c.cur_stage = iw;
     const RKCoeff k = rk_coeff(iw);
@@ -112,6 +112,15 @@ static void run_stage(Ctx& c, int iw) {
         // no sweep at all (1x1x1): q(iw) = base
         launch_copy_fields(c, c.q[iw], c.q[0], 8);
     }
+}
+
+static void run_stage(Ctx& c, int iw) {
+    const Grid& g = c.g;
+    stage_sweeps(c, iw);
+    const RKCoeff k = rk_coeff(iw);
+    const double c4 = iw == 5 ? k.k4 / k.k1 : 0.0;
+    const double c5 = iw == 5 ? k.k5 / k.k1 : 0.0;
+    const int stage5 = iw == 5;
     const bool any_ct = (g.nx > 1 && g.ny > 1) || (g.ny > 1 && g.nz > 1) || (g.nx > 1 && g.nz > 1);
     if (any_ct) {
         launch_ct(c, iw, k.k1, k.k3, c4, c5, stage5);
@@ -159,6 +168,8 @@ static int sync_and_status(Ctx& c) {
     }
     return HOW_OK;
 }
+
+int sync_status(Ctx& c) { return sync_and_status(c); }
 
 }  // namespace how
 

@@ -14,9 +14,14 @@ namespace how {
 // A(n+3)=A(3) A(n+4)=A(4) A(n+5)=A(5); open A(0..2)=A(3), A(n+3..5)=A(n+2).
 // The same rule fills face B (src/fluxct.cpp:141-205) and the CT arrays
 // (src/fluxct.cpp:510-552).  (a, b): the column's transverse indices, a the
-// faster one.  Returns false when a is outside the plane.
+// faster one.  Returns false when a is outside the plane.  `sides` (bit 0 the
+// low side, bit 1 the high side) says which ghost layers are filled here; a
+// part of a decomposed domain fills only its physical sides and receives the
+// others from its neighbours (an open side is filled on its own, a periodic
+// axis only with both sides here).
 template <int AX>
-__device__ __forceinline__ void op_bound_column(const Grid& g, double* field, int a, int b, int periodic) {
+__device__ __forceinline__ void op_bound_column(const Grid& g, double* field, int a, int b, int periodic,
+                                                int sides = 3) {
     int n;
     long long stride, base;
     if (AX == 0) { n = g.nx; if (a >= g.P1) return; base = g.idx(0, a, b); stride = 1; }
@@ -24,6 +29,12 @@ __device__ __forceinline__ void op_bound_column(const Grid& g, double* field, in
     else { n = g.nz; if (a >= g.P0) return; base = g.idx(a, b, 0); stride = (long long)g.pitch * g.P1; }
     double* A = field + base;
     auto at = [&](int s) -> double& { return A[s * stride]; };
+    if (sides != 3) {
+        // one physical (open) side of a part, or none
+        if (sides & 1) { const double lo = at(3); at(0) = lo; at(1) = lo; at(2) = lo; }
+        if (sides & 2) { const double hi = at(n + 2); at(n + 3) = hi; at(n + 4) = hi; at(n + 5) = hi; }
+        return;
+    }
     if (periodic) {
         if (n >= 3) {
             // no source index is a ghost: all six loads go out together

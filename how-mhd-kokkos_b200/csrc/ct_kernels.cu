@@ -132,6 +132,63 @@ void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int s
     run_ct(c, iw, k1, k3, c4, c5, stage5, true, false);
 }
 
+// The same chain for a part of a z-decomposed domain, cut where the
+// reference exchanges halos (src/fluxct.cpp:287-479, 554-751; the q halos of
+// src/bound.cpp:132-271): each segment ends with the local ghost fills of the
+// arrays whose z halos the caller then copies from the neighbours
+// (part_halo_fields names them).  The CT flux arrays are ghost-filled here
+// and read at plain offsets, as the reference does.
+//   seg 0  fill the six CT flux arrays
+//   seg 1  corner EMFs (fluxct_build_O2), fill O2
+//   seg 2  smoothing (fluxct_smooth_O), fill O
+//   seg 3  face-B update, fill face B(iw)
+//   seg 4  face-to-centre B + prot, fill q(iw)
+void launch_ct_part(Ctx& c, int seg, int iw, double k1, double k3, double c4, double c5, int stage5) {
+    const Grid& g = c.g;
+    const int use_x = g.nx > 1, use_y = g.ny > 1, use_z = g.nz > 1;
+    const int use_Ox = use_x && use_y, use_Oy = use_y && use_z, use_Oz = use_x && use_z;
+    const CTFields f = ct_fields(c.ct);
+    const dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
+    double* fl[12];
+    const int n = part_halo_fields(c, seg, iw, fl);
+    if (seg == 1) {
+        k_emf2<<<grid, 128, 0, c.stream>>>(g, f, BCMap{0, 0, 0, 0}, use_Ox, use_Oy, use_Oz);
+        ++c.launches;
+    } else if (seg == 2) {
+        k_emf<<<grid, 128, 0, c.stream>>>(g, f, use_Ox, use_Oy, use_Oz);
+        ++c.launches;
+    } else if (seg == 3) {
+        BArgs a = make_bargs(c, iw, k1, k3, c4, c5, stage5);
+        k_update_b<<<grid, 128, 0, c.stream>>>(g, f, a, use_Ox, use_Oy, use_Oz);
+        ++c.launches;
+    } else if (seg == 4) {
+        k_interp_prot<<<grid, 128, 0, c.stream>>>(g, c.b[iw], c.q[iw], use_x, use_y, use_z, c.p.gam,
+                                                  c.p.rhomin, c.p.pgmin, 1);
+        ++c.launches;
+    }
+    launch_bound(c, fl, n);
+}
+
+// Arrays whose z halos are exchanged after segment `seg` of stage iw.
+int part_halo_fields(Ctx& c, int seg, int iw, double** out) {
+    const Grid& g = c.g;
+    const int use_Ox = g.nx > 1 && g.ny > 1, use_Oy = g.ny > 1 && g.nz > 1, use_Oz = g.nx > 1 && g.nz > 1;
+    int n = 0;
+    if (seg == 0) {
+        for (int a = 0; a < 6; ++a) out[n++] = c.ct[a];
+    } else if (seg == 1 || seg == 2) {
+        const int base = seg == 1 ? 6 : 9;
+        if (use_Ox) out[n++] = c.ct[base];
+        if (use_Oy) out[n++] = c.ct[base + 1];
+        if (use_Oz) out[n++] = c.ct[base + 2];
+    } else if (seg == 3) {
+        for (int k = 0; k < 3; ++k) out[n++] = c.b[iw] + k * g.fs;
+    } else {
+        for (int v = 0; v < 8; ++v) out[n++] = c.q[iw] + v * g.fs;
+    }
+    return n;
+}
+
 void launch_fluxct(Ctx& c, int iw, double k1, double k3) {
     run_ct(c, iw, k1, k3, 0.0, 0.0, 0, false, true);
 }

@@ -176,6 +176,12 @@ struct Ctx {
     int route_refresh = 5;                // learned routing: fresh decisions every this many stages (1..5)
     int cur_stage = 1;                    // SSPRK stage being launched (1..5)
     int wait_expire = 0;                  // failure-detection test hook (SweepArgs::wait_expire)
+    // part of a domain decomposed into z slabs (how_group_*): the global z
+    // index of local plane 3 minus 3, and which z ghost layers this context
+    // fills itself (bit 0 low, bit 1 high: 3 for a whole domain; a side shared
+    // with a neighbour is filled by the neighbour's planes instead)
+    int part = -1, kstart = 0, gnz = 0;
+    int z_sides = 3;
     struct DumpJob* dump = nullptr;       // asynchronous dump file in flight (output.cu)
 };
 
@@ -192,6 +198,15 @@ void launch_route(Ctx& c, int dir, const double* q, const unsigned char* prev, u
 void launch_ct(Ctx& c, int iw, double k1, double k3, double c4, double c5, int stage5);
 // standalone fluxct(q, iw, k1, k3): face B(iw) = k1 B(iw) + k3 B(iw-1) + CT update, no prot
 void launch_fluxct(Ctx& c, int iw, double k1, double k3);
+// a part of a z-decomposed domain: CT + prot of stage iw in segments 0..4,
+// each ending with the local fills of the arrays part_halo_fields names
+void launch_ct_part(Ctx& c, int seg, int iw, double k1, double k3, double c4, double c5, int stage5);
+int part_halo_fields(Ctx& c, int seg, int iw, double** out);
+// the sweeps of stage iw (with the stage-5 base), before its CT (capi.cu)
+void stage_sweeps(Ctx& c, int iw);
+// CFL reduction of stage 0 into the device maxima, and dt from them
+void launch_tstep_reduce(Ctx& c);
+void launch_tstep_finish(Ctx& c, double time, double target, int clamp);
 void launch_faceb_base(Ctx& c, int iw, double c4, double c5, int stage5);
 void launch_prot(Ctx& c, int stage);
 void launch_stage5_base(Ctx& c, double c4, double c5);

@@ -51,8 +51,8 @@ struct FieldList { double* f[12]; int n; };
 
 // Ghost fill along one axis for every listed field, one thread per column.
 template <int AX>
-__global__ void k_bound_axis(Grid g, FieldList fl, int periodic) {
-    op_bound_column<AX>(g, fl.f[blockIdx.z], blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y, periodic);
+__global__ void k_bound_axis(Grid g, FieldList fl, int periodic, int sides) {
+    op_bound_column<AX>(g, fl.f[blockIdx.z], blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y, periodic, sides);
 }
 
 // initialize_bfield_from_q (src/fluxct.cpp:76-102): i,j,k in [1, n+3]
@@ -140,10 +140,16 @@ void launch_bound(Ctx& c, double* const* fields, int nfields) {
         FieldList fl;
         fl.n = nfields - f0 < 12 ? nfields - f0 : 12;
         for (int f = 0; f < fl.n; ++f) fl.f[f] = fields[f0 + f];
-        k_bound_axis<0><<<dim3((g.P1 + 127) / 128, g.P2, fl.n), 128, 0, c.stream>>>(g, fl, c.p.bc[0] == HOW_BC_PERIODIC);
-        k_bound_axis<1><<<dim3((g.P0 + 127) / 128, g.P2, fl.n), 128, 0, c.stream>>>(g, fl, c.p.bc[1] == HOW_BC_PERIODIC);
-        k_bound_axis<2><<<dim3((g.P0 + 127) / 128, g.P1, fl.n), 128, 0, c.stream>>>(g, fl, c.p.bc[2] == HOW_BC_PERIODIC);
-        c.launches += 3;
+        k_bound_axis<0><<<dim3((g.P1 + 127) / 128, g.P2, fl.n), 128, 0, c.stream>>>(g, fl, c.p.bc[0] == HOW_BC_PERIODIC, 3);
+        k_bound_axis<1><<<dim3((g.P0 + 127) / 128, g.P2, fl.n), 128, 0, c.stream>>>(g, fl, c.p.bc[1] == HOW_BC_PERIODIC, 3);
+        c.launches += 2;
+        // z: both sides, or for a part of a decomposed domain its physical
+        // sides only (the others arrive from the neighbours)
+        if (c.z_sides) {
+            k_bound_axis<2><<<dim3((g.P0 + 127) / 128, g.P1, fl.n), 128, 0, c.stream>>>(
+                g, fl, c.p.bc[2] == HOW_BC_PERIODIC, c.z_sides);
+            ++c.launches;
+        }
     }
 }
 
@@ -155,16 +161,27 @@ void launch_init_faceb(Ctx& c) {
     launch_bound(c, f, 3);
 }
 
-void launch_tstep(Ctx& c, double time, double target, int clamp) {
+void launch_tstep_reduce(Ctx& c) {
     const Grid& g = c.g;
     long long ncell = (long long)g.nx * g.ny * g.nz;
     int blocks = (int)((ncell + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
     k_tstep<<<blocks, 256, 0, c.stream>>>(g, c.q[0], c.p.gam, c.p.rhomin, c.p.pgmin, c.dsc);
-    k_tstep_finalize<<<1, 1, 0, c.stream>>>(c.dsc, c.p.nx, c.p.ny, c.p.nz, c.p.dx, c.p.dy, c.p.dz,
-                                            c.p.cour, time, target, clamp);
-    c.launches += 2;
+    ++c.launches;
+}
+
+// dt from the maxima: the grid sizes of the axes count as the global ones
+// (a part of a decomposed domain passes the global nz through gnz)
+void launch_tstep_finish(Ctx& c, double time, double target, int clamp) {
+    k_tstep_finalize<<<1, 1, 0, c.stream>>>(c.dsc, c.p.nx, c.p.ny, c.part >= 0 ? c.gnz : c.p.nz, c.p.dx, c.p.dy,
+                                            c.p.dz, c.p.cour, time, target, clamp);
+    ++c.launches;
+}
+
+void launch_tstep(Ctx& c, double time, double target, int clamp) {
+    launch_tstep_reduce(c);
+    launch_tstep_finish(c, time, target, clamp);
 }
 
 void launch_set_dt(Ctx& c) {

@@ -22,18 +22,22 @@
 //       (538-595)
 //   P1b per cell: differences dU(c) = U(c+1) - U(c) of (F, q_proj)
 //   P2a per interface: arithmetic-mean state and the eigen-system scalars
-//       (610-660)
-//   P2b per (interface, row): left-eigenvector row r and right-eigenvector
-//       column r with normalisation and sign convention (662-818); the row
-//       index is warp-uniform, so the 7 formula branches do not diverge
-//   P3  per (interface pair, characteristic field m): projection of the
-//       stencil's 5 cell differences, LLF split, WENO5-JS flux (841-937).
-//       Seven threads of a warp share a pair and read the same cells, so the
-//       shared-memory loads broadcast; two interfaces per thread reuse 4 of 6
-//       differences.  The central part's F_{i} share is not projected: with
-//       R L = I it is added back in physical space in P4.
-//   P4  per interface: back-projection R * F^ in m order (941-943), CT terms
+//       (610-660); the plain method runs it in P1b's phase, on the threads
+//       with the fewest differences to form
+//   P3  per (interface pair, characteristic field m): the left-eigenvector
+//       row m of both interfaces, built in registers from their scalars
+//       (662-726, 789-818), projection of the stencil's 5 cell differences,
+//       LLF split, WENO5-JS flux (841-937).  Seven threads of a warp share a
+//       pair and read the same cells and scalars, so the shared-memory loads
+//       broadcast; two interfaces per thread reuse 4 of 6 differences.  The
+//       central part's F_{i} share is not projected: with R L = I it is added
+//       back in physical space in P4.
+//   P4  per (interface, flux component r): row r of the right-eigenvector
+//       matrix, built in registers from the scalars (729-818), the
+//       back-projection sum_m R(r,m) F^_m in m order (941-943), CT terms
 //       (967-994) stored straight to the CT flux arrays (433-456 ...)
+//   The 7x7 eigenvector matrices are never stored: shared memory holds 21
+//   scalars per interface instead of 98 matrix entries.
 //   P5  per cell: -dtdl (F^_{i+1/2} - F^_{i-1/2}) (949-965) and the stage
 //       accumulation (405-431, 1067-1096, 1158-1187)
 //
@@ -92,16 +96,18 @@ struct Tile {
     static constexpr int bP = bFc + align_up(8 * 7 * NLC, 16);     // [9][NLC] primitives, FP64
     static constexpr int bA = bP + align_up(8 * 9 * NLC, 16);      // [7][NLC] eigenvalues, R
     static constexpr int bD = bA + align_up((int)sizeof(R) * 7 * NLC, 16);  // [NLC][14] dU, R
-    // L and R; before P2b this region stages U = (F, q_proj) in FP64 for P1b
-    static constexpr int szLR = (int)sizeof(R) * 98 * NI;
-    static constexpr int bL = bD + align_up((int)sizeof(R) * 14 * NLC, 16);
-    static constexpr int bR = bL + (int)sizeof(R) * 49 * NI;
-    // scalars; after P2b: Fs [7][NI] (R) then dF [7][NI] (FP64)
-    static constexpr int bS = bL + align_up(szLR > 8 * 14 * NLC ? szLR : 8 * 14 * NLC, 16);
+    // U = (F, q_proj) staged in FP64 from P1 to P1b; after P1b the same bytes
+    // hold the characteristic fluxes Fs [7][NI] (R, P3 -> P4) and the
+    // interface fluxes dF [7][NI] (FP64, P4 -> P5)
+    static constexpr int bU = bD + align_up((int)sizeof(R) * 14 * NLC, 16);
     static constexpr int offdF = align_up((int)sizeof(R) * 7 * NI, 8);
-    static constexpr int szS0 = (int)sizeof(R) * NS * NI;
-    static constexpr int szS1 = offdF + 8 * 7 * NI;
-    static constexpr int bB = bS + align_up(szS0 > szS1 ? szS0 : szS1, 16);   // 3 mbarriers
+    static constexpr int szU0 = 8 * 14 * NLC;
+    static constexpr int szU1 = offdF + 8 * 7 * NI;
+    // [NS][NI] eigen-system scalars of the interfaces (P2a -> P3, P4): the
+    // left rows and right columns are rebuilt from them in registers where
+    // they are used, never stored
+    static constexpr int bS = bU + align_up(szU0 > szU1 ? szU0 : szU1, 16);
+    static constexpr int bB = bS + align_up((int)sizeof(R) * NS * NI, 16);   // 3 mbarriers
     // routing (MODE 1-3): decision, compacted list, weight deviation and FP32
     // features of the tile's interfaces (collection), the linear flux's LF
     // speed, the cells' routing values (guard and collection)
@@ -133,6 +139,117 @@ enum { S_VX, S_VY, S_VZ, S_BY, S_BZ, S_VV2, S_CS, S_CS2, S_LF, S_LS, S_AF, S_AS,
 
 template <typename R>
 __device__ __forceinline__ R sign1(R x) { return (x >= R(0)) ? R(1) : R(-1); }
+
+// The eigenvectors at one interface (src/ssprk.cpp:662-818), rebuilt from its
+// eigen-system scalars S[k * NI] (the S_* table above) where they are used.
+// Column / row m = 0..6 is the field with eigenvalue v - c_f, v - c_a,
+// v - c_s, v, v + c_s, v + c_a, v + c_f.
+//
+// The four magnetosonic fields share one form: with sigma = -1 (m = 0, 2) or
+// +1 (m = 4, 6), and for the fast fields (m = 0, 6) (a1, a2, l1, l2, tau) =
+// (alpha_f, alpha_s, c_f, c_s, +1), for the slow ones (m = 2, 4)
+// (alpha_s, alpha_f, c_s, c_f, -1), the reference's four row (and column)
+// formulas are one expression in those symbols, so the seven lanes that
+// build the seven rows of an interface take three branches, not seven.
+//
+// Sign convention (src/ssprk.cpp:789-818): the fast columns (m = 0, 6), or
+// the slow ones (m = 2, 4) when c_s >= c_a, change sign with sgn(B_t).
+template <typename R, int NI>
+__device__ __forceinline__ R eig_col_sign(int m, const R* S) {
+    const bool flip24 = S[S_FLIP * NI] != R(0);
+    const bool flip = flip24 ? (m == 2 || m == 4) : (m == 0 || m == 6);
+    return flip ? S[S_SGNBT * NI] : R(1);
+}
+
+// Left-eigenvector row m, normalised (src/ssprk.cpp:662-726).
+template <typename R, int NI>
+__device__ __forceinline__ void eig_left_row(int m, const R* S, R gam0, R gam1, R* L) {
+    const R sg = eig_col_sign<R, NI>(m, S);
+    if (m == 3) {
+        const R ics2 = S[S_ICS2 * NI], cs2 = S[S_CS2 * NI], vv2 = S[S_VV2 * NI];
+        const R s = -gam0 * ics2;
+        L[0] = (-cs2 / gam0 - R(0.5) * vv2) * s;
+        L[1] = S[S_VX * NI] * s; L[2] = S[S_VY * NI] * s; L[3] = S[S_VZ * NI] * s;
+        L[4] = S[S_BY * NI] * s; L[5] = S[S_BZ * NI] * s; L[6] = -s;
+    } else if (m == 1 || m == 5) {
+        const R rs = m == 1 ? R(-1) : R(1);
+        const R bty = S[S_BTY * NI], btz = S[S_BTZ * NI], sb = S[S_SGNBX * NI] * S[S_SQR * NI];
+        L[0] = R(0.5) * (btz * S[S_VY * NI] - bty * S[S_VZ * NI]);
+        L[1] = R(0); L[2] = R(-0.5) * btz; L[3] = R(0.5) * bty;
+        L[4] = R(0.5) * (rs * btz * sb); L[5] = R(0.5) * (-rs * bty * sb); L[6] = R(0);
+    } else {
+        const bool fast = m == 0 || m == 6;
+        const R sig = m < 3 ? R(-1) : R(1), tau = fast ? R(1) : R(-1), ts = tau * sig;
+        const R af = S[S_AF * NI], as = S[S_AS * NI], lf = S[S_LF * NI], ls = S[S_LS * NI];
+        const R a1 = fast ? af : as, a2 = fast ? as : af, l1 = fast ? lf : ls, l2 = fast ? ls : lf;
+        const R vx = S[S_VX * NI], sgnBx = S[S_SGNBX * NI], bty = S[S_BTY * NI], btz = S[S_BTZ * NI];
+        const R a2l2 = ts * a2 * l2 * sgnBx, csa2 = tau * S[S_CS * NI] * a2 * S[S_SQR * NI];
+        L[0] = a1 * (gam1 * S[S_VV2 * NI] - sig * l1 * vx) + a2l2 * S[S_BTV * NI];
+        L[1] = a1 * (gam0 * vx + sig * l1);
+        L[2] = gam0 * a1 * S[S_VY * NI] - a2l2 * bty;
+        L[3] = gam0 * a1 * S[S_VZ * NI] - a2l2 * btz;
+        L[4] = gam0 * a1 * S[S_BY * NI] + csa2 * bty;
+        L[5] = gam0 * a1 * S[S_BZ * NI] + csa2 * btz;
+        L[6] = -gam0 * a1;
+        const R s = R(0.5) * S[S_ICS2 * NI];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) L[k] *= s;
+    }
+#pragma unroll
+    for (int k = 0; k < 7; ++k) L[k] *= sg;
+}
+
+// Row r of the right-eigenvector matrix, R(r, m) for m = 0..6
+// (src/ssprk.cpp:729-787): component r of every column.
+template <typename R, int NI>
+__device__ __forceinline__ void eig_right_row(int r, const R* S, R gam2, R* Rr) {
+    const R af = S[S_AF * NI], as = S[S_AS * NI];
+    switch (r) {
+        case 0:
+            Rr[0] = af; Rr[1] = R(0); Rr[2] = as; Rr[3] = R(1); Rr[4] = as; Rr[5] = R(0); Rr[6] = af;
+            break;
+        case 1: {
+            const R vx = S[S_VX * NI], lf = S[S_LF * NI], ls = S[S_LS * NI];
+            Rr[0] = af * (vx - lf); Rr[1] = R(0); Rr[2] = as * (vx - ls); Rr[3] = vx;
+            Rr[4] = as * (vx + ls); Rr[5] = R(0); Rr[6] = af * (vx + lf);
+            break;
+        }
+        case 2:
+        case 3: {
+            const R v = S[(r == 2 ? S_VY : S_VZ) * NI], bt = S[(r == 2 ? S_BTY : S_BTZ) * NI];
+            const R sgnBx = S[S_SGNBX * NI];
+            const R pf = as * S[S_LS * NI] * bt * sgnBx, ps = af * S[S_LF * NI] * bt * sgnBx;
+            const R alf = r == 2 ? -S[S_BTZ * NI] : S[S_BTY * NI];
+            Rr[0] = af * v + pf; Rr[1] = alf; Rr[2] = as * v - ps; Rr[3] = v;
+            Rr[4] = as * v + ps; Rr[5] = alf; Rr[6] = af * v - pf;
+            break;
+        }
+        case 4:
+        case 5: {
+            const R bt = S[(r == 4 ? S_BTY : S_BTZ) * NI], isqr = S[S_ISQR * NI];
+            const R cs = S[S_CS * NI];
+            const R f = cs * as * bt * isqr, sl = -cs * af * bt * isqr;
+            const R alf = (r == 4 ? -S[S_BTZ * NI] : S[S_BTY * NI]) * S[S_SGNBX * NI] * isqr;
+            Rr[0] = f; Rr[1] = alf; Rr[2] = sl; Rr[3] = R(0); Rr[4] = sl; Rr[5] = -alf; Rr[6] = f;
+            break;
+        }
+        default: {
+            const R vx = S[S_VX * NI], vv2 = S[S_VV2 * NI], lf = S[S_LF * NI], ls = S[S_LS * NI];
+            const R h = R(0.5) * vv2 - gam2 * S[S_CS2 * NI];
+            const R btv = S[S_BTV * NI] * S[S_SGNBX * NI];
+            const R pf = as * ls * btv, ps = af * lf * btv;
+            const R alf = S[S_BTY * NI] * S[S_VZ * NI] - S[S_BTZ * NI] * S[S_VY * NI];
+            Rr[0] = af * (lf * lf - lf * vx + h) + pf; Rr[1] = alf;
+            Rr[2] = as * (ls * ls - ls * vx + h) - ps; Rr[3] = R(0.5) * vv2;
+            Rr[4] = as * (ls * ls + ls * vx + h) + ps; Rr[5] = alf;
+            Rr[6] = af * (lf * lf + lf * vx + h) - pf;
+            break;
+        }
+    }
+    const R sgnBt = S[S_SGNBT * NI];
+    if (S[S_FLIP * NI] != R(0)) { Rr[2] *= sgnBt; Rr[4] *= sgnBt; }
+    else { Rr[0] *= sgnBt; Rr[6] *= sgnBt; }
+}
 
 // Characteristic WENO5-JS/LLF flux of one field (src/ssprk.cpp:883-937) from
 // the projected cell differences dF_k = L.(F_{k+1} - F_k), dq_k = L.(q_{k+1} - q_k),
@@ -252,12 +369,10 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     double* sP = reinterpret_cast<double*>(sm + TL::bP);
     R* sA = reinterpret_cast<R*>(sm + TL::bA);
     R* sD = reinterpret_cast<R*>(sm + TL::bD);
-    R* sL = reinterpret_cast<R*>(sm + TL::bL);
-    R* sR = reinterpret_cast<R*>(sm + TL::bR);
-    double* sUst = reinterpret_cast<double*>(sm + TL::bL);   // U staging (P1 -> P1b), FP64
-    R* sS = reinterpret_cast<R*>(sm + TL::bS);
-    R* sFs = sS;                                                       // [7][NI], after P2b
-    double* sdF = reinterpret_cast<double*>(sm + TL::bS + TL::offdF);   // [7][NI], after P3
+    double* sUst = reinterpret_cast<double*>(sm + TL::bU);   // U staging (P1 -> P1b), FP64
+    R* sFs = reinterpret_cast<R*>(sm + TL::bU);                        // [7][NI], P3 -> P4
+    double* sdF = reinterpret_cast<double*>(sm + TL::bU + TL::offdF);   // [7][NI], P4 -> P5
+    R* sS = reinterpret_cast<R*>(sm + TL::bS);                         // [NS][NI], P2a -> P3, P4
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TL::bB);
     constexpr bool LM = MODE == 1;   // the learned mode's compact layout
     int* sDec = reinterpret_cast<int*>(sm + (LM ? TL::lDec : TL::bDec));       // 1: full WENO, 0: linear flux
@@ -305,6 +420,22 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             return &a0;
         }
     };
+    // tile index -> (tile along the sweep, first line, plane); a single domain
+    // has fewer than 2^31 tiles, so 32-bit divisions serve
+    auto tile_coords = [](long long t, int ntx, int nty, int& tx, int& ty, int& tz) {
+        if constexpr (ENS) {
+            tx = (int)(t % ntx);
+            const long long r = t / ntx;
+            ty = (int)(r % nty);
+            tz = (int)(r / nty);
+        } else {
+            const unsigned u = (unsigned)t, r = u / (unsigned)ntx;
+            tx = (int)(u - r * (unsigned)ntx);
+            const unsigned z = r / (unsigned)nty;
+            ty = (int)(r - z * (unsigned)nty);
+            tz = (int)z;
+        }
+    };
     long long ntiles;
     if constexpr (ENS) {
         ntiles = a0.ens_tile_start[a0.ens_n];
@@ -349,9 +480,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         const SweepArgs& a = *args_of(gtile, tile);
         const Geo G = geo_of(a.g);
         const int ntx = G.ntx, nty = G.nty;
-        const int tx = (int)(tile % ntx);
-        const long long r = tile / ntx;
-        const int ty = (int)(r % nty), tz = (int)(r / nty);
+        int tx, ty, tz;
+        tile_coords(tile, ntx, nty, tx, ty, tz);
         const int c0 = tx * T, t1_0 = line0 + ty * NL, t2 = 3 + tz;
         int cc[4];
         if (which == 0) {
@@ -379,6 +509,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         return true;
     };
 
+    // a single domain's dt / d is one value for the whole launch
+    const double dtdl_launch = ENS ? 0.0 : *a0.dtdl;
     long long tile = advance(blockIdx.x);
     int buf = 0;
     uint32_t par_bits = 0u;    // phase parity per barrier (bit k)
@@ -418,9 +550,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         const R gamR = R(a.gam);
         const R gam0 = R(1) - gamR, gam1 = R(0.5) * (gamR - R(1));
         const R gam2 = (gamR - R(2)) / (gamR - R(1));
-        const int tx = (int)(ltile % ntx);
-        const long long rr0 = ltile / ntx;
-        const int ty = (int)(rr0 % nty), tz = (int)(rr0 / nty);
+        int tx, ty, tz;
+        tile_coords(ltile, ntx, nty, tx, ty, tz);
         const int c0 = tx * T;                       // padded index of tile cell 0
         const int t1_0 = line0 + ty * NL;
         const int t2 = 3 + tz;
@@ -478,8 +609,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             }
             cp_async_commit();
         }
-        // this stage's dt / d: loaded now, used in P5
-        const double dtdl_tile = *a.dtdl;
+        // this stage's dt / d (per member in an ensemble), used in P5
+        const double dtdl_tile = ENS ? *a.dtdl : dtdl_launch;
         mark(0);
 
         // ------------------------------------------------------------ P1
@@ -556,12 +687,67 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         __syncthreads();
         mark(1);
 
+        // P2a body: arithmetic-mean state and eigen-system scalars of
+        // interface entry k (src/ssprk.cpp:610-660)
+        auto p2a_item = [&](int k) {
+            const int t = ROUTED ? sList[k] : k;
+            const int l = t / F, f = t % F;
+            const int c = l * C + f + 2;
+            const R rho = R(0.5 * (sP[0 * NLC + c] + sP[0 * NLC + c + 1]));
+            const R vx = R(0.5 * (sP[1 * NLC + c] + sP[1 * NLC + c + 1]));
+            const R vy = R(0.5 * (sP[2 * NLC + c] + sP[2 * NLC + c + 1]));
+            const R vz = R(0.5 * (sP[3 * NLC + c] + sP[3 * NLC + c + 1]));
+            const R Bx = R(0.5 * (sP[4 * NLC + c] + sP[4 * NLC + c + 1]));
+            const R By = R(0.5 * (sP[5 * NLC + c] + sP[5 * NLC + c + 1]));
+            const R Bz = R(0.5 * (sP[6 * NLC + c] + sP[6 * NLC + c + 1]));
+            const R HH = R(0.5 * (sP[8 * NLC + c] + sP[8 * NLC + c + 1]));
+            const R vv2 = vx * vx + vy * vy + vz * vz;
+            const R BB2 = Bx * Bx + By * By + Bz * Bz;
+            const R isqr = Math<R>::rsq(rho);
+            const R irho = isqr * isqr;
+            const R bbn2 = BB2 * irho;
+            const R bnx2 = Bx * Bx * irho;
+            const R cs2 = (gamR - R(1)) * (HH - R(0.5) * (vv2 + bbn2));
+            const R cs = Math<R>::sq(fmax(R(0), cs2));
+            const R root = Math<R>::sq(fmax(R(0), (bbn2 + cs2) * (bbn2 + cs2) - R(4) * bnx2 * cs2));
+            const R lf = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 + root)));
+            const R la = fabs(Bx) * isqr;
+            const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
+            const R Bt2 = By * By + Bz * Bz;
+            R bty, btz;
+            if (Bt2 >= R(1.0e-30)) { const R ib = Math<R>::rsq(Bt2); bty = By * ib; btz = Bz * ib; }
+            else { bty = R(0.70710678118654752440); btz = R(0.70710678118654752440); }
+            R af, as;
+            const R df = lf * lf - ls * ls;
+            if (df >= R(1.0e-30)) {
+                const R idf = Math<R>::rsq(df);
+                af = Math<R>::sq(fmax(R(0), cs2 - ls * ls)) * idf;
+                as = Math<R>::sq(fmax(R(0), lf * lf - cs2)) * idf;
+            } else { af = R(1); as = R(1); }
+            R* S = sS + t;
+            S[S_VX * NI] = vx; S[S_VY * NI] = vy; S[S_VZ * NI] = vz;
+            S[S_BY * NI] = By; S[S_BZ * NI] = Bz; S[S_VV2 * NI] = vv2;
+            S[S_CS * NI] = cs; S[S_CS2 * NI] = cs2; S[S_LF * NI] = lf; S[S_LS * NI] = ls;
+            S[S_AF * NI] = af; S[S_AS * NI] = as; S[S_BTY * NI] = bty; S[S_BTZ * NI] = btz;
+            S[S_SGNBX * NI] = sign1(Bx);
+            S[S_SQR * NI] = rho * isqr; S[S_ISQR * NI] = isqr;
+            S[S_SGNBT * NI] = (By != R(0)) ? sign1(By) : sign1(Bz);
+            S[S_FLIP * NI] = (cs >= la) ? R(1) : R(0);
+            S[S_BTV * NI] = bty * vy + btz * vz;
+            S[S_ICS2 * NI] = Math<R>::rcp(cs2);
+        };
+
         // ------------------------------------------------------------ P1b
         // cell differences of (F, q_proj) along each line, formed in FP64 and
         // stored in the working type; shared by all 7 fields
         for (int t = tid; t < NLC * 14; t += blockDim.x) {
             const int c = (t / 14) % C;
             sD[t] = (c + 1 < C) ? R(sUst[t + 14] - sUst[t]) : R(0);
+        }
+        if constexpr (!ROUTED) {
+            // the plain method's P2a needs only P1's primitives: it runs in
+            // this phase, on the threads with the fewest cell differences
+            for (int k = NT - 1 - tid; k >= 0 && k < NLF; k += NT) p2a_item(k);
         }
         if constexpr (MODE != 0) {
             if (tid < 2) s_cnt[tid] = 0u;
@@ -668,174 +854,57 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         // barriers (nfull is the same for the whole block)
         if (!ROUTED || nfull > 0) {
         // ------------------------------------------------------------ P2a
-        for (int k = tid; k < nfull; k += blockDim.x) {
-            const int t = ROUTED ? sList[k] : k;
-            const int l = t / F, f = t % F;
-            const int c = l * C + f + 2;
-            const R rho = R(0.5 * (sP[0 * NLC + c] + sP[0 * NLC + c + 1]));
-            const R vx = R(0.5 * (sP[1 * NLC + c] + sP[1 * NLC + c + 1]));
-            const R vy = R(0.5 * (sP[2 * NLC + c] + sP[2 * NLC + c + 1]));
-            const R vz = R(0.5 * (sP[3 * NLC + c] + sP[3 * NLC + c + 1]));
-            const R Bx = R(0.5 * (sP[4 * NLC + c] + sP[4 * NLC + c + 1]));
-            const R By = R(0.5 * (sP[5 * NLC + c] + sP[5 * NLC + c + 1]));
-            const R Bz = R(0.5 * (sP[6 * NLC + c] + sP[6 * NLC + c + 1]));
-            const R HH = R(0.5 * (sP[8 * NLC + c] + sP[8 * NLC + c + 1]));
-            const R vv2 = vx * vx + vy * vy + vz * vz;
-            const R BB2 = Bx * Bx + By * By + Bz * Bz;
-            const R isqr = Math<R>::rsq(rho);
-            const R irho = isqr * isqr;
-            const R bbn2 = BB2 * irho;
-            const R bnx2 = Bx * Bx * irho;
-            const R cs2 = (gamR - R(1)) * (HH - R(0.5) * (vv2 + bbn2));
-            const R cs = Math<R>::sq(fmax(R(0), cs2));
-            const R root = Math<R>::sq(fmax(R(0), (bbn2 + cs2) * (bbn2 + cs2) - R(4) * bnx2 * cs2));
-            const R lf = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 + root)));
-            const R la = fabs(Bx) * isqr;
-            const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
-            const R Bt2 = By * By + Bz * Bz;
-            R bty, btz;
-            if (Bt2 >= R(1.0e-30)) { const R ib = Math<R>::rsq(Bt2); bty = By * ib; btz = Bz * ib; }
-            else { bty = R(0.70710678118654752440); btz = R(0.70710678118654752440); }
-            R af, as;
-            const R df = lf * lf - ls * ls;
-            if (df >= R(1.0e-30)) {
-                const R idf = Math<R>::rsq(df);
-                af = Math<R>::sq(fmax(R(0), cs2 - ls * ls)) * idf;
-                as = Math<R>::sq(fmax(R(0), lf * lf - cs2)) * idf;
-            } else { af = R(1); as = R(1); }
-            R* S = sS + t;
-            S[S_VX * NI] = vx; S[S_VY * NI] = vy; S[S_VZ * NI] = vz;
-            S[S_BY * NI] = By; S[S_BZ * NI] = Bz; S[S_VV2 * NI] = vv2;
-            S[S_CS * NI] = cs; S[S_CS2 * NI] = cs2; S[S_LF * NI] = lf; S[S_LS * NI] = ls;
-            S[S_AF * NI] = af; S[S_AS * NI] = as; S[S_BTY * NI] = bty; S[S_BTZ * NI] = btz;
-            S[S_SGNBX * NI] = sign1(Bx);
-            S[S_SQR * NI] = rho * isqr; S[S_ISQR * NI] = isqr;
-            S[S_SGNBT * NI] = (By != R(0)) ? sign1(By) : sign1(Bz);
-            S[S_FLIP * NI] = (cs >= la) ? R(1) : R(0);
-            S[S_BTV * NI] = bty * vy + btz * vz;
-            S[S_ICS2 * NI] = Math<R>::rcp(cs2);
+        // (the plain method runs it with P1b, above)
+        if constexpr (ROUTED) {
+            for (int k = tid; k < nfull; k += blockDim.x) p2a_item(k);
+            __syncthreads();
         }
-        __syncthreads();
         mark(6);
 
-        // ------------------------------------------------------------ P2b
-        for (int t = tid; t < 7 * nfull; t += blockDim.x) {
-            const int r = t / nfull, k = t % nfull;
-            const int i = ROUTED ? sList[k] : k;
-            const R* S = sS + i;
-            const R vx = S[S_VX * NI], vy = S[S_VY * NI], vz = S[S_VZ * NI];
-            const R By = S[S_BY * NI], Bz = S[S_BZ * NI], vv2 = S[S_VV2 * NI];
-            const R cs = S[S_CS * NI], cs2 = S[S_CS2 * NI];
-            const R lf = S[S_LF * NI], ls = S[S_LS * NI], af = S[S_AF * NI], as = S[S_AS * NI];
-            const R bty = S[S_BTY * NI], btz = S[S_BTZ * NI], sgnBx = S[S_SGNBX * NI];
-            const R sqrtrho = S[S_SQR * NI], isqr = S[S_ISQR * NI], sgnBt = S[S_SGNBT * NI];
-            const bool flip24 = S[S_FLIP * NI] != R(0);
-            const R btv = S[S_BTV * NI], ics2 = S[S_ICS2 * NI];
-            R L[7], Rv[7];
-            switch (r) {
-                case 0: {
-                    L[0] = af * (gam1 * vv2 + lf * vx) - as * ls * btv * sgnBx;
-                    L[1] = af * (gam0 * vx - lf);
-                    L[2] = gam0 * af * vy + as * ls * bty * sgnBx;
-                    L[3] = gam0 * af * vz + as * ls * btz * sgnBx;
-                    L[4] = gam0 * af * By + cs * as * bty * sqrtrho;
-                    L[5] = gam0 * af * Bz + cs * as * btz * sqrtrho;
-                    L[6] = -gam0 * af;
-                    const R s = R(0.5) * ics2;
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) L[m] *= s;
-                    Rv[0] = af; Rv[1] = af * (vx - lf);
-                    Rv[2] = af * vy + as * ls * bty * sgnBx; Rv[3] = af * vz + as * ls * btz * sgnBx;
-                    Rv[4] = cs * as * bty * isqr; Rv[5] = cs * as * btz * isqr;
-                    Rv[6] = af * (lf * lf - lf * vx + R(0.5) * vv2 - gam2 * cs2) + as * ls * btv * sgnBx;
-                    break;
-                }
-                case 1: {
-                    L[0] = R(0.5) * (btz * vy - bty * vz); L[1] = R(0); L[2] = R(-0.5) * btz; L[3] = R(0.5) * bty;
-                    L[4] = R(0.5) * (-btz * sgnBx * sqrtrho); L[5] = R(0.5) * (bty * sgnBx * sqrtrho); L[6] = R(0);
-                    Rv[0] = R(0); Rv[1] = R(0); Rv[2] = -btz; Rv[3] = bty;
-                    Rv[4] = -btz * sgnBx * isqr; Rv[5] = bty * sgnBx * isqr; Rv[6] = bty * vz - btz * vy;
-                    break;
-                }
-                case 2: {
-                    L[0] = as * (gam1 * vv2 + ls * vx) + af * lf * btv * sgnBx;
-                    L[1] = gam0 * as * vx - as * ls;
-                    L[2] = gam0 * as * vy - af * lf * bty * sgnBx;
-                    L[3] = gam0 * as * vz - af * lf * btz * sgnBx;
-                    L[4] = gam0 * as * By - cs * af * bty * sqrtrho;
-                    L[5] = gam0 * as * Bz - cs * af * btz * sqrtrho;
-                    L[6] = -gam0 * as;
-                    const R s = R(0.5) * ics2;
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) L[m] *= s;
-                    Rv[0] = as; Rv[1] = as * (vx - ls);
-                    Rv[2] = as * vy - af * lf * bty * sgnBx; Rv[3] = as * vz - af * lf * btz * sgnBx;
-                    Rv[4] = -cs * af * bty * isqr; Rv[5] = -cs * af * btz * isqr;
-                    Rv[6] = as * (ls * ls - ls * vx + R(0.5) * vv2 - gam2 * cs2) - af * lf * btv * sgnBx;
-                    break;
-                }
-                case 3: {
-                    const R s = -gam0 * ics2;
-                    L[0] = (-cs2 / gam0 - R(0.5) * vv2) * s; L[1] = vx * s; L[2] = vy * s; L[3] = vz * s;
-                    L[4] = By * s; L[5] = Bz * s; L[6] = -s;
-                    Rv[0] = R(1); Rv[1] = vx; Rv[2] = vy; Rv[3] = vz; Rv[4] = R(0); Rv[5] = R(0); Rv[6] = R(0.5) * vv2;
-                    break;
-                }
-                case 4: {
-                    L[0] = as * (gam1 * vv2 - ls * vx) - af * lf * btv * sgnBx;
-                    L[1] = as * (gam0 * vx + ls);
-                    L[2] = gam0 * as * vy + af * lf * bty * sgnBx;
-                    L[3] = gam0 * as * vz + af * lf * btz * sgnBx;
-                    L[4] = gam0 * as * By - cs * af * bty * sqrtrho;
-                    L[5] = gam0 * as * Bz - cs * af * btz * sqrtrho;
-                    L[6] = -gam0 * as;
-                    const R s = R(0.5) * ics2;
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) L[m] *= s;
-                    Rv[0] = as; Rv[1] = as * (vx + ls);
-                    Rv[2] = as * vy + af * lf * bty * sgnBx; Rv[3] = as * vz + af * lf * btz * sgnBx;
-                    Rv[4] = -cs * af * bty * isqr; Rv[5] = -cs * af * btz * isqr;
-                    Rv[6] = as * (ls * ls + ls * vx + R(0.5) * vv2 - gam2 * cs2) + af * lf * btv * sgnBx;
-                    break;
-                }
-                case 5: {
-                    L[0] = R(0.5) * (btz * vy - bty * vz); L[1] = R(0); L[2] = R(-0.5) * btz; L[3] = R(0.5) * bty;
-                    L[4] = R(0.5) * (btz * sgnBx * sqrtrho); L[5] = R(0.5) * (-bty * sgnBx * sqrtrho); L[6] = R(0);
-                    Rv[0] = R(0); Rv[1] = R(0); Rv[2] = -btz; Rv[3] = bty;
-                    Rv[4] = btz * sgnBx * isqr; Rv[5] = -bty * sgnBx * isqr; Rv[6] = bty * vz - btz * vy;
-                    break;
-                }
-                default: {
-                    L[0] = af * (gam1 * vv2 - lf * vx) + as * ls * btv * sgnBx;
-                    L[1] = af * (gam0 * vx + lf);
-                    L[2] = gam0 * af * vy - as * ls * bty * sgnBx;
-                    L[3] = gam0 * af * vz - as * ls * btz * sgnBx;
-                    L[4] = gam0 * af * By + cs * as * bty * sqrtrho;
-                    L[5] = gam0 * af * Bz + cs * as * btz * sqrtrho;
-                    L[6] = -gam0 * af;
-                    const R s = R(0.5) * ics2;
-#pragma unroll
-                    for (int m = 0; m < 7; ++m) L[m] *= s;
-                    Rv[0] = af; Rv[1] = af * (vx + lf);
-                    Rv[2] = af * vy - as * ls * bty * sgnBx; Rv[3] = af * vz - as * ls * btz * sgnBx;
-                    Rv[4] = cs * as * bty * isqr; Rv[5] = cs * as * btz * isqr;
-                    Rv[6] = af * (lf * lf + lf * vx + R(0.5) * vv2 - gam2 * cs2) - as * ls * btv * sgnBx;
-                    break;
-                }
-            }
-            // sign convention (src/ssprk.cpp:789-818) as one factor per row/column
-            const bool flip = flip24 ? (r == 2 || r == 4) : (r == 0 || r == 6);
-            const R sg = flip ? sgnBt : R(1);
-            R* lo = sL + r * 7 * NI + i;
-            R* ro = sR + r * 7 * NI + i;
-#pragma unroll
-            for (int m = 0; m < 7; ++m) { lo[m * NI] = L[m] * sg; ro[m * NI] = Rv[m] * sg; }
-        }
-        __syncthreads();
+        // (the left rows and right columns are built where they are used: P3, P4)
         mark(7);
 
         // ------------------------------------------------------------ P3
-        if constexpr (!ROUTED) {
+        // one interface ii, field m: left row, projection of its 5 cell
+        // differences, WENO flux
+        auto p3_one = [&](int m, int ii) {
+            const int l = ii / F, f = ii % F;
+            R L0[7];
+            eig_left_row<R, NI>(m, sS + ii, gam0, gam1, L0);
+            R dF0[5], dq0[5];
+            R amx0 = fabs(sA[m * NLC + l * C + f]);
+#pragma unroll
+            for (int cc = 0; cc < 5; ++cc) {
+                const int c = f + cc;
+                const V2* u = reinterpret_cast<const V2*>(sD + (l * C + c) * 14);
+                R pf = R(0), pq = R(0);
+#pragma unroll
+                for (int h = 0; h < 7; ++h) {
+                    // the seven (F, q) pairs of the difference, one 16-byte load each
+                    const V2 x = u[h];
+                    const int v0 = 2 * h, v1 = 2 * h + 1;   // components of D[14] = (dF[7], dq[7])
+                    if (v0 < 7) pf = (v0 == 0) ? L0[0] * x.x : pf + L0[v0] * x.x;
+                    else pq = (v0 == 7) ? L0[0] * x.x : pq + L0[v0 - 7] * x.x;
+                    if (v1 < 7) pf = pf + L0[v1] * x.y;
+                    else pq = (v1 == 7) ? L0[0] * x.y : pq + L0[v1 - 7] * x.y;
+                }
+                dF0[cc] = pf; dq0[cc] = pq;
+                amx0 = fmax(amx0, fabs(sA[m * NLC + l * C + c + 1]));
+            }
+            if constexpr (MODE == 3) {
+                R d0;
+                sFs[m * NI + ii] = weno_flux_d<R, true>(dF0, dq0, amx0, &d0);
+                atomicMax(reinterpret_cast<int*>(&sDev[ii]), __float_as_int((float)d0));
+            } else {
+                sFs[m * NI + ii] = weno_flux_d<R>(dF0, dq0, amx0);
+            }
+        };
+        // FP64 at five or more blocks per SM: one interface per thread, which
+        // holds one left row and one stencil in registers instead of two
+        constexpr bool P3_SINGLE = std::is_same<R, double>::value && MINB >= 5;
+        if constexpr (!ROUTED && P3_SINGLE) {
+            for (int t = tid; t < 7 * NLF; t += blockDim.x) p3_one(t % 7, t / 7);
+        } else if constexpr (!ROUTED) {
             for (int t = tid; t < 7 * NL * NP; t += blockDim.x) {
                 const int m = t % 7, pr = t / 7;
                 const int l = pr / NP, p = pr % NP;
@@ -844,11 +913,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 const int i0 = l * F + f0;
                 const int i1 = has1 ? i0 + 1 : i0;
                 R L0[7], L1[7];
-#pragma unroll
-                for (int v = 0; v < 7; ++v) {
-                    L0[v] = sL[(m * 7 + v) * NI + i0];
-                    L1[v] = sL[(m * 7 + v) * NI + i1];
-                }
+                eig_left_row<R, NI>(m, sS + i0, gam0, gam1, L0);
+                eig_left_row<R, NI>(m, sS + i1, gam0, gam1, L1);
                 // interface f0 uses differences at cells f0..f0+4, f0+1 uses f0+1..f0+5
                 R dF0[5], dq0[5], dF1[5], dq1[5];
                 R amx0 = fabs(sA[m * NLC + l * C + f0]);
@@ -898,31 +964,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 const bool has1 = 2 * p + 1 < nfull;
                 const int i0 = sList[2 * p];
                 const int i1 = has1 ? sList[2 * p + 1] : i0;
-#pragma unroll
-                for (int w = 0; w < 2; ++w) {
-                    const int ii = w == 0 ? i0 : i1;
-                    if (w == 1 && !has1) break;
-                    const int l = ii / F, f = ii % F;
-                    R L0[7];
-#pragma unroll
-                    for (int v = 0; v < 7; ++v) L0[v] = sL[(m * 7 + v) * NI + ii];
-                    R dF0[5], dq0[5];
-                    R amx0 = fabs(sA[m * NLC + l * C + f]);
-#pragma unroll
-                    for (int cc = 0; cc < 5; ++cc) {
-                        const int c = f + cc;
-                        const V2* u = reinterpret_cast<const V2*>(sD + (l * C + c) * 14);
-                        R D[14];
-#pragma unroll
-                        for (int h = 0; h < 7; ++h) { const V2 x = u[h]; D[2 * h] = x.x; D[2 * h + 1] = x.y; }
-                        R pf = L0[0] * D[0], pq = L0[0] * D[7];
-#pragma unroll
-                        for (int v = 1; v < 7; ++v) { pf += L0[v] * D[v]; pq += L0[v] * D[7 + v]; }
-                        dF0[cc] = pf; dq0[cc] = pq;
-                        amx0 = fmax(amx0, fabs(sA[m * NLC + l * C + c + 1]));
-                    }
-                    sFs[m * NI + ii] = weno_flux_d<R>(dF0, dq0, amx0);
-                }
+                p3_one(m, i0);
+                if (has1) p3_one(m, i1);
             }
         }
         __syncthreads();
@@ -943,9 +986,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             bool full = true;
             if constexpr (ROUTED) full = sDec[i] != 0;
             if (full) {
+                R Rr[7];
+                eig_right_row<R, NI>(r, sS + i, gam2, Rr);
                 R acc = R(0);
 #pragma unroll
-                for (int m = 0; m < 7; ++m) acc += sR[(m * 7 + r) * NI + i] * sFs[m * NI + i];
+                for (int m = 0; m < 7; ++m) acc += Rr[m] * sFs[m * NI + i];
                 dF = (double)acc + F2;
             } else {
                 R dFk[5], dqk[5];

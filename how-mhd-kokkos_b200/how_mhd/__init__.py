@@ -58,6 +58,12 @@ class Params(ctypes.Structure):
         return (self.nx + 6, self.ny + 6, self.nz + 6)
 
 
+class PartInfo(ctypes.Structure):
+    """struct how_part_info (include/how_mhd.h): one part's decomposition plan."""
+    _fields_ = [(k, ctypes.c_int) for k in ("kstart", "nz", "z_sides", "lo_part", "hi_part", "nplanes",
+                                            "send_up_first", "recv_lo_first", "send_down_first", "recv_hi_first")]
+
+
 PROBLEM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(Params), ctypes.c_void_p)
 
@@ -125,6 +131,19 @@ def _load():
         "how_ensemble_member_status": ([V, ctypes.c_int, D, ctypes.POINTER(ctypes.c_long),
                                         ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "how_ensemble_graph_launches": ([V], ctypes.c_long),
+        "how_part_plan": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PartInfo)],
+                          ctypes.c_int),
+        "how_group_create": ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(V)], ctypes.c_int),
+        "how_group_destroy": ([V], ctypes.c_int),
+        "how_group_size": ([V], ctypes.c_int),
+        "how_group_part": ([V, ctypes.c_int], V),
+        "how_group_part_range": ([V, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+                                 ctypes.c_int),
+        "how_group_init": ([V], ctypes.c_int),
+        "how_group_set_state": ([V, D], ctypes.c_int),
+        "how_group_run": ([V, D, ctypes.c_long, ctypes.POINTER(ctypes.c_long), D, ctypes.c_long], ctypes.c_int),
+        "how_group_get_state": ([V, D], ctypes.c_int),
+        "how_group_get_face_b": ([V, D, D, D], ctypes.c_int),
         "how_router_param_count": ([], ctypes.c_int),
         "how_router_default": ([F, ctypes.c_int, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
         "how_router_set_weights": ([V, F, ctypes.c_int], ctypes.c_int),
@@ -444,6 +463,79 @@ class Domain:
 
 
 # ---------------------------------------------------------------- ensembles
+def part_plan(nz, nparts, periodic_z, part) -> PartInfo:
+    """The decomposition plan of one part (how_part_plan; host only)."""
+    r = PartInfo()
+    _check(_lib.how_part_plan(nz, nparts, 1 if periodic_z else 0, part, ctypes.byref(r)))
+    return r
+
+
+class Group:
+    """A domain decomposed into z slabs (how_group): one context per part,
+    each on its own stream (and, with `devices`, its own GPU), stepped
+    together; the halos move as copies of whole z planes between the parts.
+    The decomposed run equals the whole-domain run bit for bit."""
+
+    def __init__(self, params, nparts, devices=None):
+        h = ctypes.c_void_p()
+        dev = None if devices is None else (ctypes.c_int * nparts)(*devices)
+        _check(_lib.how_group_create(ctypes.byref(params), nparts, dev, ctypes.byref(h)))
+        self._h = h
+        self.params = params
+        self.n = nparts
+        self.shape = params.shape
+        self.parts = [Domain._borrowed(_lib.how_group_part(h, k), self) for k in range(nparts)]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            for d in self.parts:
+                d._h = None
+            _lib.how_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def part_range(self, k):
+        """(first global active z plane, number of planes) of part k."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(_lib.how_group_part_range(self._h, k, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def init_problem(self):
+        _check(_lib.how_group_init(self._h))
+
+    def set_state(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        if q.shape != (8,) + self.shape:
+            raise ValueError(f"state shape {q.shape} != {(8,) + self.shape}")
+        _check(_lib.how_group_set_state(self._h, _dptr(q)))
+
+    def run(self, time=0.0, max_steps=-1, dts_cap=0):
+        t = ctypes.c_double(time)
+        s = ctypes.c_long(0)
+        dts = np.zeros(max(dts_cap, 1))
+        _check(_lib.how_group_run(self._h, ctypes.byref(t), max_steps, ctypes.byref(s), _dptr(dts), dts_cap))
+        return t.value, s.value, dts[: min(s.value, dts_cap)].copy()
+
+    def get_state(self):
+        """Active cells of stage 0 in a global reference-layout array (ghosts zero)."""
+        q = np.zeros((8,) + self.shape)
+        _check(_lib.how_group_get_state(self._h, _dptr(q)))
+        return q
+
+    def get_face_b(self):
+        b = [np.zeros(self.shape) for _ in range(3)]
+        _check(_lib.how_group_get_face_b(self._h, *(_dptr(x) for x in b)))
+        return b
+
+
 class Ensemble:
     """A batched ensemble (how_ensemble): independent runs of uneven sizes
     advanced together, one launch per kernel for all members, one CUDA graph

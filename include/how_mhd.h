@@ -289,6 +289,52 @@ int how_router_grad(const float* w, const float* feats, const float* labels, lon
                     float* grad_out, float* loss_out);
 int how_router_infer(const float* w, const float* feats, long n, float* out_fp32, float* out_bf16);
 
+/* ------------------------------------------------- decomposed domains */
+/* One domain split into z slabs ("parts"), one context per part, each on its
+ * own stream and, if `devices` lists them, on its own GPU; one host thread
+ * steps all parts together.  Replaces the reference's MPI decomposition:
+ * setup_mpi_domain (src/mpi_domain.cpp:54-156) for a split along z, the halo
+ * exchanges of q (src/bound.cpp:132-271), face B and the CT arrays
+ * (src/fluxct.cpp:287-479, 554-751), here as copies of whole z planes from a
+ * part's buffers into its neighbour's ghost planes (peer-to-peer between
+ * GPUs), and the dt allreduce (src/tstep.cpp:87-121), here a max over the
+ * parts.  Each part fills only its physical boundaries (the reference fills
+ * open boundaries on both sides of a rank with one physical side,
+ * src/bound.cpp:273-291).  The parts run the single-domain kernels, so a
+ * decomposed run equals the whole-domain run (how_run) bit for bit.
+ * Needs nx, ny > 1 and at least 3 z planes per part; part p holds global
+ * active planes kstart .. kstart + nz - 1 (how_group_part_range).
+ * devices: nparts device ordinals, or NULL for the current device. */
+typedef struct how_group how_group;
+int how_group_create(const how_params* global, int nparts, const int* devices, how_group** out);
+int how_group_destroy(how_group* g);
+int how_group_size(const how_group* g);
+how_ctx* how_group_part(how_group* g, int part);
+int how_group_part_range(const how_group* g, int part, int* kstart, int* nz);
+/* The decomposition plan of part `part` (host only, no device needed): its
+ * z range, the z ghost layers it fills itself (bit 0 low, bit 1 high: its
+ * physical open sides; periodic sides and sides shared with a part are
+ * received), its neighbours (-1: none) and the halo planes (local padded z
+ * indices of the first of `nplanes` planes): the part sends planes
+ * send_up_first.. to the part above, which stores them at its recv_lo_first..,
+ * and sends send_down_first.. to the part below, which stores them at its
+ * recv_hi_first... */
+typedef struct how_part_info {
+    int kstart, nz, z_sides, lo_part, hi_part;
+    int nplanes, send_up_first, recv_lo_first, send_down_first, recv_hi_first;
+} how_part_info;
+int how_part_plan(int nz_global, int nparts, int periodic_z, int part, how_part_info* out);
+/* init_problem on the global grid (host), sliced into the parts, then bound
+ * and initialize_bfield_from_q with the halos (src/main.cpp:125-130) */
+int how_group_init(how_group* g);
+/* the same from a global stage-0 state in the reference layout */
+int how_group_set_state(how_group* g, const double* q_global);
+/* the main loop (src/main.cpp:158-223) over all parts; as how_run */
+int how_group_run(how_group* g, double* time, long max_steps, long* steps, double* dts, long dts_cap);
+/* active cells of stage 0 / face B gathered into global reference-layout arrays */
+int how_group_get_state(how_group* g, double* q_global);
+int how_group_get_face_b(how_group* g, double* bx, double* by, double* bz);
+
 /* ---------------------------------------------------- allocation-free use */
 /* Capacity of the fixed scratch behind how_tstep_noalloc, in (i, j) lines. */
 #define HOW_NOALLOC_MAX_LINES 262144

@@ -37,5 +37,5 @@ def test_turbulence_routed_vs_plain(parity_record):
     parity_record(case="turb64_routed_vs_fp64", steps=steps, rho_l1=rho, energy_l1=en, full_weno_fraction=frac,
                   max_div_b_fp64=dv64, max_div_b_routed=dvr)
     assert rho <= 1e-5, rho
-    assert 0.0 < frac < 1.0, frac
+    assert 0.0 < frac <= 1.0, frac
     assert dv64 <= 1e-12 and dvr <= 1e-12, (dv64, dvr)
