@@ -164,7 +164,6 @@ __device__ __forceinline__ R eig_col_sign(int m, const R* S) {
 // Left-eigenvector row m, normalised (src/ssprk.cpp:662-726).
 template <typename R, int NI>
 __device__ __forceinline__ void eig_left_row(int m, const R* S, R gam0, R gam1, R* L) {
-    const R sg = eig_col_sign<R, NI>(m, S);
     if (m == 3) {
         const R ics2 = S[S_ICS2 * NI], cs2 = S[S_CS2 * NI], vv2 = S[S_VV2 * NI];
         const R s = -gam0 * ics2;
@@ -191,12 +190,11 @@ __device__ __forceinline__ void eig_left_row(int m, const R* S, R gam0, R gam1, 
         L[4] = gam0 * a1 * S[S_BY * NI] + csa2 * bty;
         L[5] = gam0 * a1 * S[S_BZ * NI] + csa2 * btz;
         L[6] = -gam0 * a1;
-        const R s = R(0.5) * S[S_ICS2 * NI];
+        // normalisation and the sign convention (only magnetosonic rows flip)
+        const R s = R(0.5) * S[S_ICS2 * NI] * eig_col_sign<R, NI>(m, S);
 #pragma unroll
         for (int k = 0; k < 7; ++k) L[k] *= s;
     }
-#pragma unroll
-    for (int k = 0; k < 7; ++k) L[k] *= sg;
 }
 
 // Row r of the right-eigenvector matrix, R(r, m) for m = 0..6
@@ -344,6 +342,10 @@ __device__ __forceinline__ constexpr int perm_of(int dir, int v) {
          : dir == 1 ? (v == 1 ? 2 : v == 2 ? 3 : v == 3 ? 1 : v == 4 ? 5 : v == 5 ? 6 : v == 6 ? 4 : v)
                     : (v == 1 ? 3 : v == 2 ? 1 : v == 3 ? 2 : v == 4 ? 6 : v == 5 ? 4 : v == 6 ? 5 : v);
 }
+
+#ifndef HOW_P2A_IN_P1
+#define HOW_P2A_IN_P1 1
+#endif
 
 constexpr uint32_t kWaitLimit = 1u << 26;   // bounded TMA wait (~seconds), then flag and skip
 
@@ -613,30 +615,112 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         const double dtdl_tile = ENS ? *a.dtdl : dtdl_launch;
         mark(0);
 
+        // P2a: eigen-system scalars of interface t from the arithmetic mean of
+        // its two cells' primitives (src/ssprk.cpp:610-660)
+        auto p2a_core = [&](int t, double mrho, double mvx, double mvy, double mvz, double mBx, double mBy,
+                            double mBz, double mHH) {
+            const R rho = R(mrho), vx = R(mvx), vy = R(mvy), vz = R(mvz);
+            const R Bx = R(mBx), By = R(mBy), Bz = R(mBz), HH = R(mHH);
+            const R vv2 = vx * vx + vy * vy + vz * vz;
+            const R BB2 = Bx * Bx + By * By + Bz * Bz;
+            const R isqr = Math<R>::rsq(rho);
+            const R irho = isqr * isqr;
+            const R bbn2 = BB2 * irho;
+            const R bnx2 = Bx * Bx * irho;
+            const R cs2 = (gamR - R(1)) * (HH - R(0.5) * (vv2 + bbn2));
+            const R cs = Math<R>::sq(fmax(R(0), cs2));
+            const R root = Math<R>::sq(fmax(R(0), (bbn2 + cs2) * (bbn2 + cs2) - R(4) * bnx2 * cs2));
+            const R lf = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 + root)));
+            const R la = fabs(Bx) * isqr;
+            const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
+            const R Bt2 = By * By + Bz * Bz;
+            R bty, btz;
+            if (Bt2 >= R(1.0e-30)) { const R ib = Math<R>::rsq(Bt2); bty = By * ib; btz = Bz * ib; }
+            else { bty = R(0.70710678118654752440); btz = R(0.70710678118654752440); }
+            R af, as;
+            const R df = lf * lf - ls * ls;
+            if (df >= R(1.0e-30)) {
+                const R idf = Math<R>::rsq(df);
+                af = Math<R>::sq(fmax(R(0), cs2 - ls * ls)) * idf;
+                as = Math<R>::sq(fmax(R(0), lf * lf - cs2)) * idf;
+            } else { af = R(1); as = R(1); }
+            R* S = sS + t;
+            S[S_VX * NI] = vx; S[S_VY * NI] = vy; S[S_VZ * NI] = vz;
+            S[S_BY * NI] = By; S[S_BZ * NI] = Bz; S[S_VV2 * NI] = vv2;
+            S[S_CS * NI] = cs; S[S_CS2 * NI] = cs2; S[S_LF * NI] = lf; S[S_LS * NI] = ls;
+            S[S_AF * NI] = af; S[S_AS * NI] = as; S[S_BTY * NI] = bty; S[S_BTZ * NI] = btz;
+            S[S_SGNBX * NI] = sign1(Bx);
+            S[S_SQR * NI] = rho * isqr; S[S_ISQR * NI] = isqr;
+            S[S_SGNBT * NI] = (By != R(0)) ? sign1(By) : sign1(Bz);
+            S[S_FLIP * NI] = (cs >= la) ? R(1) : R(0);
+            S[S_BTV * NI] = bty * vy + btz * vz;
+            S[S_ICS2 * NI] = Math<R>::rcp(cs2);
+        };
+        // the same from the primitives P1 stored (routed modes: list entry k)
+        auto p2a_item = [&](int k) {
+            const int t = ROUTED ? sList[k] : k;
+            const int c = (t / F) * C + t % F + 2;
+            p2a_core(t, 0.5 * (sP[0 * NLC + c] + sP[0 * NLC + c + 1]), 0.5 * (sP[1 * NLC + c] + sP[1 * NLC + c + 1]),
+                     0.5 * (sP[2 * NLC + c] + sP[2 * NLC + c + 1]), 0.5 * (sP[3 * NLC + c] + sP[3 * NLC + c + 1]),
+                     0.5 * (sP[4 * NLC + c] + sP[4 * NLC + c + 1]), 0.5 * (sP[5 * NLC + c] + sP[5 * NLC + c + 1]),
+                     0.5 * (sP[6 * NLC + c] + sP[6 * NLC + c + 1]), 0.5 * (sP[8 * NLC + c] + sP[8 * NLC + c + 1]));
+        };
+
         // ------------------------------------------------------------ P1
         // two threads per cell: the first forms primitives and fluxes, the
         // second the eigenvalues (both from the same primitive arithmetic)
-        for (int tt = tid; tt < 2 * NLC; tt += blockDim.x) {
+        // primit (src/ssprk.cpp:479-512) of tile cell (l, cc): v from the
+        // unfloored density, floors on rho and p with E recomputed
+        struct Prim { double rho, irho, vx, vy, vz, Bx, By, Bz, EE, pg, vv2, BB2, Mx, My, Mz; };
+        auto primit = [&](int l, int cc) -> Prim {
+            Prim o;
+            const double DD = qraw(0, l, cc);
+            o.Mx = qraw(1, l, cc); o.My = qraw(2, l, cc); o.Mz = qraw(3, l, cc);
+            o.Bx = qraw(4, l, cc); o.By = qraw(5, l, cc); o.Bz = qraw(6, l, cc);
+            o.EE = qraw(7, l, cc);
+            o.rho = DD;
+            o.irho = 1.0 / o.rho;
+            o.vx = o.Mx * o.irho; o.vy = o.My * o.irho; o.vz = o.Mz * o.irho;
+            o.vv2 = o.vx * o.vx + o.vy * o.vy + o.vz * o.vz;
+            o.BB2 = o.Bx * o.Bx + o.By * o.By + o.Bz * o.Bz;
+            o.pg = (gam - 1.0) * (o.EE - 0.5 * (o.rho * o.vv2 + o.BB2));
+            if (o.rho < a.rhomin || o.pg < a.pgmin) {
+                o.rho = fmax(a.rhomin, o.rho);
+                o.pg = fmax(a.pgmin, o.pg);
+                o.EE = o.pg / (gam - 1.0) + 0.5 * (o.rho * o.vv2 + o.BB2);
+                o.irho = 1.0 / o.rho;
+            }
+            return o;
+        };
+        // The plain method's P2a (per interface) needs only the primitives of
+        // its two cells: its threads form them from the raw tile themselves and
+        // run alongside P1, on threads P1 leaves idle.
+        constexpr bool P2A_IN_P1 = !ROUTED && HOW_P2A_IN_P1;
+        constexpr int NP1 = P2A_IN_P1 ? 2 * NLC + NLF : 2 * NLC;
+        for (int tt = tid; tt < NP1; tt += blockDim.x) {
+            if (P2A_IN_P1 && tt >= 2 * NLC) {
+                const int k = tt - 2 * NLC;
+                const int l = k / F, f = k % F;
+                // the means 0.5 (a + b), accumulated as 0.5 a + 0.5 b (the same
+                // value: halving is exact) so one cell's primitives are live at a time
+                double m[8];
+#pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const Prim u = primit(l, f + 2 + side);
+                    const double h[8] = {u.rho, u.vx, u.vy, u.vz, u.Bx, u.By, u.Bz, (u.EE + u.pg) * u.irho};
+#pragma unroll
+                    for (int v = 0; v < 8; ++v) m[v] = side == 0 ? 0.5 * h[v] : m[v] + 0.5 * h[v];
+                }
+                p2a_core(k, m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7]);
+                continue;
+            }
             const bool eig = tt >= NLC;
             const int t = eig ? tt - NLC : tt;
             const int l = t / C, cc = t % C;
-            const double DD = qraw(0, l, cc), Mx = qraw(1, l, cc), My = qraw(2, l, cc);
-            const double Mz = qraw(3, l, cc), Bx = qraw(4, l, cc), By = qraw(5, l, cc);
-            const double Bz = qraw(6, l, cc);
-            double EE = qraw(7, l, cc);
-            // primit (src/ssprk.cpp:479-512): v from the unfloored density
-            double rho = DD;
-            double irho = 1.0 / rho;
-            const double vx = Mx * irho, vy = My * irho, vz = Mz * irho;
-            const double vv2 = vx * vx + vy * vy + vz * vz;
-            const double BB2 = Bx * Bx + By * By + Bz * Bz;
-            double pg = (gam - 1.0) * (EE - 0.5 * (rho * vv2 + BB2));
-            if (rho < a.rhomin || pg < a.pgmin) {
-                rho = fmax(a.rhomin, rho);
-                pg = fmax(a.pgmin, pg);
-                EE = pg / (gam - 1.0) + 0.5 * (rho * vv2 + BB2);
-                irho = 1.0 / rho;
-            }
+            const Prim u = primit(l, cc);
+            const double rho = u.rho, irho = u.irho, vx = u.vx, vy = u.vy, vz = u.vz;
+            const double Bx = u.Bx, By = u.By, Bz = u.Bz, EE = u.EE, pg = u.pg, vv2 = u.vv2, BB2 = u.BB2;
+            const double Mx = u.Mx, My = u.My, Mz = u.Mz;
             if (!eig) {
                 const double HH = (EE + pg) * irho;
                 sP[0 * NLC + t] = rho; sP[1 * NLC + t] = vx; sP[2 * NLC + t] = vy; sP[3 * NLC + t] = vz;
@@ -679,63 +763,15 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 const R la = Math<R>::sq(fmax(R(0), bnx2));
                 const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
                 const R vxR = R(vx);
-                sA[0 * NLC + t] = vxR - lf; sA[1 * NLC + t] = vxR - la; sA[2 * NLC + t] = vxR - ls;
-                sA[3 * NLC + t] = vxR;      sA[4 * NLC + t] = vxR + ls; sA[5 * NLC + t] = vxR + la;
-                sA[6 * NLC + t] = vxR + lf;
+                // |lambda_m|: every reader takes the magnitude (the LLF speeds)
+                sA[0 * NLC + t] = fabs(vxR - lf); sA[1 * NLC + t] = fabs(vxR - la);
+                sA[2 * NLC + t] = fabs(vxR - ls); sA[3 * NLC + t] = fabs(vxR);
+                sA[4 * NLC + t] = fabs(vxR + ls); sA[5 * NLC + t] = fabs(vxR + la);
+                sA[6 * NLC + t] = fabs(vxR + lf);
             }
         }
         __syncthreads();
         mark(1);
-
-        // P2a body: arithmetic-mean state and eigen-system scalars of
-        // interface entry k (src/ssprk.cpp:610-660)
-        auto p2a_item = [&](int k) {
-            const int t = ROUTED ? sList[k] : k;
-            const int l = t / F, f = t % F;
-            const int c = l * C + f + 2;
-            const R rho = R(0.5 * (sP[0 * NLC + c] + sP[0 * NLC + c + 1]));
-            const R vx = R(0.5 * (sP[1 * NLC + c] + sP[1 * NLC + c + 1]));
-            const R vy = R(0.5 * (sP[2 * NLC + c] + sP[2 * NLC + c + 1]));
-            const R vz = R(0.5 * (sP[3 * NLC + c] + sP[3 * NLC + c + 1]));
-            const R Bx = R(0.5 * (sP[4 * NLC + c] + sP[4 * NLC + c + 1]));
-            const R By = R(0.5 * (sP[5 * NLC + c] + sP[5 * NLC + c + 1]));
-            const R Bz = R(0.5 * (sP[6 * NLC + c] + sP[6 * NLC + c + 1]));
-            const R HH = R(0.5 * (sP[8 * NLC + c] + sP[8 * NLC + c + 1]));
-            const R vv2 = vx * vx + vy * vy + vz * vz;
-            const R BB2 = Bx * Bx + By * By + Bz * Bz;
-            const R isqr = Math<R>::rsq(rho);
-            const R irho = isqr * isqr;
-            const R bbn2 = BB2 * irho;
-            const R bnx2 = Bx * Bx * irho;
-            const R cs2 = (gamR - R(1)) * (HH - R(0.5) * (vv2 + bbn2));
-            const R cs = Math<R>::sq(fmax(R(0), cs2));
-            const R root = Math<R>::sq(fmax(R(0), (bbn2 + cs2) * (bbn2 + cs2) - R(4) * bnx2 * cs2));
-            const R lf = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 + root)));
-            const R la = fabs(Bx) * isqr;
-            const R ls = Math<R>::sq(fmax(R(0), R(0.5) * (bbn2 + cs2 - root)));
-            const R Bt2 = By * By + Bz * Bz;
-            R bty, btz;
-            if (Bt2 >= R(1.0e-30)) { const R ib = Math<R>::rsq(Bt2); bty = By * ib; btz = Bz * ib; }
-            else { bty = R(0.70710678118654752440); btz = R(0.70710678118654752440); }
-            R af, as;
-            const R df = lf * lf - ls * ls;
-            if (df >= R(1.0e-30)) {
-                const R idf = Math<R>::rsq(df);
-                af = Math<R>::sq(fmax(R(0), cs2 - ls * ls)) * idf;
-                as = Math<R>::sq(fmax(R(0), lf * lf - cs2)) * idf;
-            } else { af = R(1); as = R(1); }
-            R* S = sS + t;
-            S[S_VX * NI] = vx; S[S_VY * NI] = vy; S[S_VZ * NI] = vz;
-            S[S_BY * NI] = By; S[S_BZ * NI] = Bz; S[S_VV2 * NI] = vv2;
-            S[S_CS * NI] = cs; S[S_CS2 * NI] = cs2; S[S_LF * NI] = lf; S[S_LS * NI] = ls;
-            S[S_AF * NI] = af; S[S_AS * NI] = as; S[S_BTY * NI] = bty; S[S_BTZ * NI] = btz;
-            S[S_SGNBX * NI] = sign1(Bx);
-            S[S_SQR * NI] = rho * isqr; S[S_ISQR * NI] = isqr;
-            S[S_SGNBT * NI] = (By != R(0)) ? sign1(By) : sign1(Bz);
-            S[S_FLIP * NI] = (cs >= la) ? R(1) : R(0);
-            S[S_BTV * NI] = bty * vy + btz * vz;
-            S[S_ICS2 * NI] = Math<R>::rcp(cs2);
-        };
 
         // ------------------------------------------------------------ P1b
         // cell differences of (F, q_proj) along each line, formed in FP64 and
@@ -743,11 +779,6 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         for (int t = tid; t < NLC * 14; t += blockDim.x) {
             const int c = (t / 14) % C;
             sD[t] = (c + 1 < C) ? R(sUst[t + 14] - sUst[t]) : R(0);
-        }
-        if constexpr (!ROUTED) {
-            // the plain method's P2a needs only P1's primitives: it runs in
-            // this phase, on the threads with the fewest cell differences
-            for (int k = NT - 1 - tid; k >= 0 && k < NLF; k += NT) p2a_item(k);
         }
         if constexpr (MODE != 0) {
             if (tid < 2) s_cnt[tid] = 0u;
@@ -786,9 +817,9 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             // Lax-Friedrichs speed of the linear flux: the stencil's largest |lambda|
             auto row_amx = [&](int t) {
                 const int cb = (t / F) * C + t % F;
-                R amx = fmax(fabs(sA[0 * NLC + cb]), fabs(sA[6 * NLC + cb]));
+                R amx = fmax(sA[0 * NLC + cb], sA[6 * NLC + cb]);
 #pragma unroll
-                for (int k = 1; k < 6; ++k) amx = fmax(amx, fmax(fabs(sA[0 * NLC + cb + k]), fabs(sA[6 * NLC + cb + k])));
+                for (int k = 1; k < 6; ++k) amx = fmax(amx, fmax(sA[0 * NLC + cb + k], sA[6 * NLC + cb + k]));
                 sAmx[t] = amx;
             };
             if constexpr (MODE == 1) {
@@ -854,8 +885,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         // barriers (nfull is the same for the whole block)
         if (!ROUTED || nfull > 0) {
         // ------------------------------------------------------------ P2a
-        // (the plain method runs it with P1b, above)
-        if constexpr (ROUTED) {
+        // (the plain method runs it with P1, above)
+        if constexpr (!P2A_IN_P1) {
             for (int k = tid; k < nfull; k += blockDim.x) p2a_item(k);
             __syncthreads();
         }
@@ -872,7 +903,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             R L0[7];
             eig_left_row<R, NI>(m, sS + ii, gam0, gam1, L0);
             R dF0[5], dq0[5];
-            R amx0 = fabs(sA[m * NLC + l * C + f]);
+            R amx0 = sA[m * NLC + l * C + f];
 #pragma unroll
             for (int cc = 0; cc < 5; ++cc) {
                 const int c = f + cc;
@@ -889,7 +920,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     else pq = (v1 == 7) ? L0[0] * x.y : pq + L0[v1 - 7] * x.y;
                 }
                 dF0[cc] = pf; dq0[cc] = pq;
-                amx0 = fmax(amx0, fabs(sA[m * NLC + l * C + c + 1]));
+                amx0 = fmax(amx0, sA[m * NLC + l * C + c + 1]);
             }
             if constexpr (MODE == 3) {
                 R d0;
@@ -917,8 +948,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 eig_left_row<R, NI>(m, sS + i1, gam0, gam1, L1);
                 // interface f0 uses differences at cells f0..f0+4, f0+1 uses f0+1..f0+5
                 R dF0[5], dq0[5], dF1[5], dq1[5];
-                R amx0 = fabs(sA[m * NLC + l * C + f0]);
-                R amx1 = fabs(sA[m * NLC + l * C + (f0 + 1 < C ? f0 + 1 : C - 1)]);
+                R amx0 = sA[m * NLC + l * C + f0];
+                R amx1 = sA[m * NLC + l * C + (f0 + 1 < C ? f0 + 1 : C - 1)];
 #pragma unroll
                 for (int cc = 0; cc < 6; ++cc) {
                     int c = f0 + cc;
@@ -927,7 +958,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     R D[14];
 #pragma unroll
                     for (int h = 0; h < 7; ++h) { const V2 x = u[h]; D[2 * h] = x.x; D[2 * h + 1] = x.y; }
-                    const R av = fabs(sA[m * NLC + l * C + (c + 1)]);
+                    const R av = sA[m * NLC + l * C + (c + 1)];
                     if (cc <= 4) {
                         R pf = L0[0] * D[0], pq = L0[0] * D[7];
 #pragma unroll

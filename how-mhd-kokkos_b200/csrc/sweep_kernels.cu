@@ -4,8 +4,6 @@
 // collection}.
 #include "sweep_core.cuh"
 
-#include <cstdlib>
-
 namespace how {
 
 namespace {
@@ -121,30 +119,21 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     }
     // instantiations: {fp64, mixed} x {plain, learned, guard-only}; label
     // collection runs the FP64 method
-    static const int xv64 = getenv("HOW_XV64") ? atoi(getenv("HOW_XV64")) : 4;
-    static const int xv32 = getenv("HOW_XV32") ? atoi(getenv("HOW_XV32")) : 6;
+    // Blocks per SM (the launch bound that caps registers): six for the plain
+    // FP64 sweep (80 registers, one interface per thread in P3), seven for
+    // the mixed ones (72 registers); measured at 256^3 against 4/5 and 6/8.
 #define HOW_SWEEP_CASES(D)                                                                              \
     do {                                                                                                \
         using S = SweepShape<D>;                                                                        \
         if (mode == 3) { launch_one<D, S::NL, S::T, 128, double, 3, 3>(c, a); break; }                  \
         if (mixed) {                                                                                    \
-            if (mode == 1) {                                                                            \
-                if (xv32 == 8) launch_one<D, S::NL, S::T, 128, float, 8, 1>(c, a);                      \
-                else if (xv32 == 7) launch_one<D, S::NL, S::T, 128, float, 7, 1>(c, a);                 \
-                else launch_one<D, S::NL, S::T, 128, float, 6, 1>(c, a);                                \
-            }                                                                                           \
+            if (mode == 1) launch_one<D, S::NL, S::T, 128, float, 7, 1>(c, a);                          \
             else if (mode == 2) launch_one<D, S::NL, S::T, 128, float, 5, 2>(c, a);                     \
-            else {                                                                                      \
-                if (xv32 == 8) launch_one<D, S::NL, S::T, 128, float, 8, 0>(c, a);                      \
-                else if (xv32 == 7) launch_one<D, S::NL, S::T, 128, float, 7, 0>(c, a);                 \
-                else launch_one<D, S::NL, S::T, 128, float, 6, 0>(c, a);                                \
-            }                                                                                           \
+            else launch_one<D, S::NL, S::T, 128, float, 7, 0>(c, a);                                    \
         } else {                                                                                        \
             if (mode == 1) launch_one<D, S::NL, S::T, 128, double, 3, 1>(c, a);                         \
             else if (mode == 2) launch_one<D, S::NL, S::T, 128, double, 3, 2>(c, a);                    \
-            else if (xv64 == 6) launch_one<D, S::NL, S::T, 128, double, 6, 0>(c, a);                    \
-            else if (xv64 == 5) launch_one<D, S::NL, S::T, 128, double, 5, 0>(c, a);                    \
-            else launch_one<D, S::NL, S::T, 128, double, 4, 0>(c, a);                                   \
+            else launch_one<D, S::NL, S::T, 128, double, 6, 0>(c, a);                                   \
         }                                                                                               \
     } while (0)
     if (dir == 0) HOW_SWEEP_CASES(0);
