@@ -49,14 +49,11 @@ int main(int argc, char** argv) {
     }
     std::printf("dtout = %g\noutput step = 0 time = 0\n", dtout);
     for (int out = 1; out <= p.nt; ++out) {
-        // run one output interval: how_run stops at the interval end because
-        // the next target is reached; run it with a per-interval tend.
-        how_params q = p;
-        (void)q;
+        // the interval is advanced one how_run step at a time, until the
+        // time reaches its end (how_run clamps the last step to it,
+        // src/main.cpp:170-172), so each output lands on its time
         long steps = 0;
         std::vector<double> dts(1);
-        // advance until this interval's end (how_run honours all intervals up
-        // to tend; stop it at the interval by step-wise calls)
         const double target = dtout * out;
         while (time < target) {
             long s = 0;

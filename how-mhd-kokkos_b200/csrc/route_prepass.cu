@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kRouteThreads, 4) k_route_x(const __grid_const
             for (int k = 0; k < 6; ++k)
                 sc[k] = StencilCell{cv[warp][lane + k][0], cv[warp][lane + k][1], cv[warp][lane + k][2],
                                     cv[warp][lane + k][3], cv[warp][lane + k][4]};
-            guard = router_features(sc, (float)a.prev[face], (float)a.rhomin, (float)a.pgmin, a.guard_jump,
+            guard = router_features(sc, 0.0f /* prior-stage feature held at 0 */, (float)a.rhomin, (float)a.pgmin, a.guard_jump,
                                     a.guard_floor, ft, &flat);
         }
         route_decide(S, a, warp, lane, ft, flat, guard, live, face);
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const __grid_constant__
             const long long face = rl + iface + 2;
             if (live) {
                 win[5] = route_cell(a.q, g.fs, line + (long long)(iface + 5) * stride, DIR, a.gam, a.rhomin, a.pgmin);
-                guard = router_features(win, (float)a.prev[face], (float)a.rhomin, (float)a.pgmin, a.guard_jump,
+                guard = router_features(win, 0.0f /* prior-stage feature held at 0 */, (float)a.rhomin, (float)a.pgmin, a.guard_jump,
                                         a.guard_floor, ft, &flat);
 #pragma unroll
                 for (int k = 0; k < 5; ++k) win[k] = win[k + 1];

@@ -114,7 +114,8 @@ struct Tile {
     static constexpr int bDec = bB + 32;                          // [NLF] int
     static constexpr int bList = bDec + align_up(4 * NLF, 16);    // [NLF] int
     static constexpr int bDev = bList + align_up(4 * NLF, 16);    // [NLF] float (bits)
-    static constexpr int bFt = bDev + align_up(4 * NLF, 16);      // [NLF][6] float
+    static constexpr int bFlx = bDev + align_up(4 * NLF, 16);     // [NLF] float (bits): flux departure
+    static constexpr int bFt = bFlx + align_up(4 * NLF, 16);      // [NLF][6] float
     static constexpr int bAmx = bFt + align_up(4 * 6 * NLF, 16);  // [NLF] R: linear-flux LF speed
     static constexpr int bCF = bAmx + align_up((int)sizeof(R) * NLF, 16);   // [5][NLC] float cell features
     static constexpr int bDecW = bCF + align_up(4 * 5 * NLC, 16);  // [NL][F+2] int: fetched decisions
@@ -380,6 +381,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     int* sDec = reinterpret_cast<int*>(sm + (LM ? TL::lDec : TL::bDec));       // 1: full WENO, 0: linear flux
     int* sList = reinterpret_cast<int*>(sm + (LM ? TL::lList : TL::bList));    // full-WENO interfaces
     float* sDev = reinterpret_cast<float*>(sm + TL::bDev);      // weight deviation (collect)
+    float* sFlx = reinterpret_cast<float*>(sm + TL::bFlx);      // flux departure (collect)
     float* sFt = reinterpret_cast<float*>(sm + TL::bFt);        // features (collect)
     R* sAmx = reinterpret_cast<R*>(sm + (LM ? TL::lAmx : TL::bAmx));           // per interface: max |lambda_0|, |lambda_6|
     float* sCF = reinterpret_cast<float*>(sm + (LM ? TL::lCF : TL::bCF));      // per cell: rho, p, |B|, |v|, c_f
@@ -808,9 +810,9 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     sc[k] = StencilCell{sCF[0 * NLC + cc], sCF[1 * NLC + cc], sCF[2 * NLC + cc], sCF[3 * NLC + cc],
                                         sCF[4 * NLC + cc]};
                 }
-                const int iface = c0 + f;
-                prior = 1.0f;
-                if (line_ok(l) && iface <= n) prior = (float)a.route_prev[rline(l) + (iface + 2)];
+                // the prior-stage feature is held at 0: fed back from the
+                // network's own decisions it locked smooth flows at full WENO
+                prior = 0.0f;
                 return router_features(sc, prior, (float)a.rhomin, (float)a.pgmin, a.guard_jump, a.guard_floor, ft,
                                        &flat);
             };
@@ -862,11 +864,12 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                     bool flat;
                     float prior;
                     const bool guard = row_features(t, ft, flat, prior);
-                    if constexpr (MODE == 2) row_amx(t);
+                    row_amx(t);
                     if constexpr (MODE == 3) {
 #pragma unroll
                         for (int k = 0; k < kRouterNF; ++k) sFt[t * 6 + k] = ft[k];
                         sDev[t] = 0.0f;
+                        sFlx[t] = 0.0f;
                     }
                     sDec[t] = MODE == 3 ? 1 : (guard ? 1 : 0);
                     if constexpr (MODE == 2) {
@@ -1023,6 +1026,38 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
 #pragma unroll
                 for (int m = 0; m < 7; ++m) acc += Rr[m] * sFs[m * NI + i];
                 dF = (double)acc + F2;
+                if constexpr (MODE == 3) {
+                    // label collection: what routing this face to the cheap
+                    // flux would change -- dt/dx |F_full - F_linear| for this
+                    // component, relative to the local size of its conserved
+                    // variable (density; rho (|v| + c) for momentum; sqrt(rho) c
+                    // for the field; the total energy), with
+                    // c^2 = (gam p + B^2) / rho at the mean state
+                    R dFk[5], dqk[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) {
+                        const int cc = l * C + f + k;
+                        dFk[k] = sD[cc * 14 + r];
+                        dqk[k] = sD[cc * 14 + 7 + r];
+                    }
+                    const double lin = (double)linear_flux_d<R>(dFk, dqk, sAmx[i]);
+                    const double rho = 0.5 * (sP[c] + sP[c + 1]);
+                    const double vx = 0.5 * (sP[NLC + c] + sP[NLC + c + 1]);
+                    const double vy = 0.5 * (sP[2 * NLC + c] + sP[2 * NLC + c + 1]);
+                    const double vz = 0.5 * (sP[3 * NLC + c] + sP[3 * NLC + c + 1]);
+                    const double bx = 0.5 * (sP[4 * NLC + c] + sP[4 * NLC + c + 1]);
+                    const double by = 0.5 * (sP[5 * NLC + c] + sP[5 * NLC + c + 1]);
+                    const double bz = 0.5 * (sP[6 * NLC + c] + sP[6 * NLC + c + 1]);
+                    const double pg = 0.5 * (sP[7 * NLC + c] + sP[7 * NLC + c + 1]);
+                    const double v2 = vx * vx + vy * vy + vz * vz, b2 = bx * bx + by * by + bz * bz;
+                    const double cs = sqrt((gam * pg + b2) / rho);
+                    const double scale = r == 0 ? rho
+                                       : r < 4 ? rho * (sqrt(v2) + cs)
+                                       : r < 6 ? sqrt(rho) * cs
+                                       : pg / (gam - 1.0) + 0.5 * rho * v2 + 0.5 * b2;
+                    const float dv = (float)(dtdl_tile * fabs((double)acc - lin) / scale);
+                    if (dv > 0.0f) atomicMax(reinterpret_cast<int*>(&sFlx[i]), __float_as_int(dv));
+                }
             } else {
                 R dFk[5], dqk[5];
 #pragma unroll
@@ -1063,26 +1098,31 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                         a.route_next[o] = (unsigned char)(full ? 1 : 0);
                         atomicAdd(&s_cnt[full ? 0 : 1], 1u);
                     }
-                    if constexpr (MODE == 3) {
-                        a.route_next[o] = (unsigned char)(sDev[i] > 0.1f ? 1 : 0);
-                        // sampled tiles: a hash of the tile index, so the
-                        // sample does not alias with the tile grid
-                        const unsigned long long hs = (unsigned long long)tile * 0x9E3779B97F4A7C15ull;
-                        if ((unsigned int)(hs >> 32) % a.collect_every == 0u) {
-                            const unsigned int slot = atomicAdd(a.collect_n, 1u);
-                            if (slot < a.collect_cap) {
-                                float* rec = a.collect + 8ull * slot;
-#pragma unroll
-                                for (int k = 0; k < 6; ++k) rec[k] = sFt[i * 6 + k];
-                                rec[6] = sDev[i] > 0.1f ? 1.0f : 0.0f;
-                                rec[7] = sDev[i];
-                            }
-                        }
-                    }
                 }
             }
         }
         __syncthreads();
+        if constexpr (MODE == 3) {
+            // the records of the tile's owned faces, once every component's
+            // flux departure is in (sampled tiles: a hash of the tile index,
+            // so the sample does not alias with the tile grid)
+            const unsigned long long hs = (unsigned long long)tile * 0x9E3779B97F4A7C15ull;
+            const bool sampled = (unsigned int)(hs >> 32) % a.collect_every == 0u;
+            for (int i = tid; i < NLF; i += blockDim.x) {
+                const int l = i / F, f = i % F, iface = c0 + f;
+                if (!(line_ok(l) && iface <= n && (f < T || iface == n))) continue;
+                a.route_next[rline(l) + (iface + 2)] = 0;
+                if (!sampled) continue;
+                const unsigned int slot = atomicAdd(a.collect_n, 1u);
+                if (slot < a.collect_cap) {
+                    float* rec = a.collect + 8ull * slot;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) rec[k] = sFt[i * 6 + k];
+                    rec[6] = sDev[i];
+                    rec[7] = sFlx[i];
+                }
+            }
+        }
         if constexpr (ROUTED) {
             if (tid == 0) {
                 atomicAdd(&a.route_count[0], (unsigned long long)s_cnt[0]);

@@ -442,7 +442,10 @@ class Domain:
         self._collect_cap = capacity
 
     def collect_end(self):
-        """Records (n, 8): 6 features, label, max weight departure."""
+        """Records (n, 8): 6 features, the largest departure of the nonlinear
+        WENO weights from the linear ones, and the flux departure (what the
+        cheap flux would change: dt/dx |F_full - F_linear| over the local size
+        of the conserved variable, largest component)."""
         cap = getattr(self, "_collect_cap", 0)
         out = np.zeros((max(cap, 1), 8), np.float32)
         n = ctypes.c_uint(0)

@@ -278,7 +278,13 @@ int how_router_stats(how_ctx* ctx, unsigned long long* full, unsigned long long*
  * precomputed flat logit -- or guarded) */
 int how_router_stats4(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap,
                       unsigned long long* mma_groups, unsigned long long* flat_groups, int reset);
-/* Label collection from the plain FP64 method (records of 8 floats). */
+/* Label collection from the plain FP64 method: records of 8 floats per
+ * sampled interface -- the 6 router features (the prior-stage feature is held
+ * at 0), the largest departure of the nonlinear WENO weights from the linear
+ * ones over the 7 fields, and the flux departure, dt/dx |F_full - F_linear|
+ * over the local size of the conserved variable (rho; rho (|v| + c);
+ * sqrt(rho) c; E), largest component: what routing the face to the cheap flux
+ * would change in one stage. */
 int how_collect_begin(how_ctx* ctx, unsigned int capacity, unsigned int every);
 int how_collect_end(how_ctx* ctx, float* out, unsigned int cap, unsigned int* n);
 /* Hand-written GPU training (FP32, Adam) of w in place, its gradient, and

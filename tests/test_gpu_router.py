@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import router_ref as rr
-from howtest import active
+from howtest import active, rel_l1
 
 pytestmark = pytest.mark.gpu
 
@@ -84,9 +84,11 @@ def test_collect_labels_from_plain_solver():
     # face once (a face shared by two tiles is recorded by one)
     assert len(rec) == 2 * 5 * 2 * 65 * 64
     assert np.isfinite(rec).all()
-    assert set(np.unique(rec[:, 6])) == {0.0, 1.0}
-    assert ((rec[:, 6] > 0.5) == (rec[:, 7] > 0.1)).all()
-    assert set(np.unique(rec[:, 5])) <= {0.0, 1.0}
+    # the weight departure lies in [0, 1]; the flux departure is >= 0, and
+    # positive somewhere in the vortex
+    assert (rec[:, 6] >= 0).all() and (rec[:, 6] <= 1).all() and (rec[:, 6] > 0.1).any()
+    assert (rec[:, 7] >= 0).all() and rec[:, 7].max() > 0
+    assert (rec[:, 5] == 0).all()   # the prior-stage feature is held at 0
     assert np.isfinite(ref).all()
 
 
@@ -121,11 +123,11 @@ def test_routed_all_full_equals_plain(prob, n, kw):
         b = d.get_state(0)
         full, cheap = d.router_stats()
     assert cheap == 0 and full > 0
-    aa, bb = active(a, *n), active(b, *n)
-    for v in range(8):
-        s = np.abs(aa[v]).sum()
-        if s > 0:
-            assert np.abs(bb[v] - aa[v]).sum() <= 1e-13 * s, v
+    # the two paths compile separately and may contract products into FMAs
+    # differently: equal to round-off, with components that are round-off
+    # noise themselves (Mz of the 2-D vortex) measured against their vector
+    err = rel_l1(active(b, *n), active(a, *n))
+    assert np.all(err <= 1e-13), err
 
 
 def test_routed_all_linear_converges_to_plain_on_alfven():
