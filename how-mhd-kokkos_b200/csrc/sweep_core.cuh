@@ -22,14 +22,14 @@
 //       (538-595)
 //   P1b per cell: differences dU(c) = U(c+1) - U(c) of (F, q_proj)
 //   P2a per interface: arithmetic-mean state and the eigen-system scalars
-//       (610-660); the plain method runs it in P1b's phase, on the threads
-//       with the fewest differences to form
-//   P3  per (interface pair, characteristic field m): the left-eigenvector
-//       row m of both interfaces, built in registers from their scalars
+//       (610-660)
+//   P3  per (interface, characteristic field m): the left-eigenvector row m,
+//       built in registers from the interface's scalars
 //       (662-726, 789-818), projection of the stencil's 5 cell differences,
-//       LLF split, WENO5-JS flux (841-937).  Seven threads of a warp share a
-//       pair and read the same cells and scalars, so the shared-memory loads
-//       broadcast; two interfaces per thread reuse 4 of 6 differences.  The
+//       LLF split, WENO5-JS flux (841-937).  Seven threads of a warp share an
+//       interface and read the same cells and scalars, so the shared-memory
+//       loads broadcast (below five blocks per SM a thread takes two
+//       interfaces and reuses 4 of their 6 differences).  The
 //       central part's F_{i} share is not projected: with R L = I it is added
 //       back in physical space in P4.
 //   P4  per (interface, flux component r): row r of the right-eigenvector
@@ -344,10 +344,6 @@ __device__ __forceinline__ constexpr int perm_of(int dir, int v) {
                     : (v == 1 ? 3 : v == 2 ? 1 : v == 3 ? 2 : v == 4 ? 6 : v == 5 ? 4 : v == 6 ? 5 : v);
 }
 
-#ifndef HOW_P2A_IN_P1
-#define HOW_P2A_IN_P1 1
-#endif
-
 constexpr uint32_t kWaitLimit = 1u << 26;   // bounded TMA wait (~seconds), then flag and skip
 
 // MODE 0: plain method.  1: learned routing (network + guard).  2: guard-only
@@ -658,7 +654,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             S[S_BTV * NI] = bty * vy + btz * vz;
             S[S_ICS2 * NI] = Math<R>::rcp(cs2);
         };
-        // the same from the primitives P1 stored (routed modes: list entry k)
+        // entry k of the interface list (every interface in the plain method),
+        // from the primitives P1 stored
         auto p2a_item = [&](int k) {
             const int t = ROUTED ? sList[k] : k;
             const int c = (t / F) * C + t % F + 2;
@@ -694,28 +691,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             }
             return o;
         };
-        // The plain method's P2a (per interface) needs only the primitives of
-        // its two cells: its threads form them from the raw tile themselves and
-        // run alongside P1, on threads P1 leaves idle.
-        constexpr bool P2A_IN_P1 = !ROUTED && HOW_P2A_IN_P1;
-        constexpr int NP1 = P2A_IN_P1 ? 2 * NLC + NLF : 2 * NLC;
-        for (int tt = tid; tt < NP1; tt += blockDim.x) {
-            if (P2A_IN_P1 && tt >= 2 * NLC) {
-                const int k = tt - 2 * NLC;
-                const int l = k / F, f = k % F;
-                // the means 0.5 (a + b), accumulated as 0.5 a + 0.5 b (the same
-                // value: halving is exact) so one cell's primitives are live at a time
-                double m[8];
-#pragma unroll
-                for (int side = 0; side < 2; ++side) {
-                    const Prim u = primit(l, f + 2 + side);
-                    const double h[8] = {u.rho, u.vx, u.vy, u.vz, u.Bx, u.By, u.Bz, (u.EE + u.pg) * u.irho};
-#pragma unroll
-                    for (int v = 0; v < 8; ++v) m[v] = side == 0 ? 0.5 * h[v] : m[v] + 0.5 * h[v];
-                }
-                p2a_core(k, m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7]);
-                continue;
-            }
+        for (int tt = tid; tt < 2 * NLC; tt += blockDim.x) {
             const bool eig = tt >= NLC;
             const int t = eig ? tt - NLC : tt;
             const int l = t / C, cc = t % C;
@@ -888,11 +864,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         // barriers (nfull is the same for the whole block)
         if (!ROUTED || nfull > 0) {
         // ------------------------------------------------------------ P2a
-        // (the plain method runs it with P1, above)
-        if constexpr (!P2A_IN_P1) {
-            for (int k = tid; k < nfull; k += blockDim.x) p2a_item(k);
-            __syncthreads();
-        }
+        for (int k = tid; k < nfull; k += blockDim.x) p2a_item(k);
+        __syncthreads();
         mark(6);
 
         // (the left rows and right columns are built where they are used: P3, P4)
