@@ -91,7 +91,8 @@ struct Tile {
     static constexpr int NS = 21;                   // eigen-system scalars per interface
     // byte offsets (base 128-byte aligned; TMA destinations on 128 B)
     static constexpr int bQ = 0;                                   // 2 x [8][..] raw conserved, FP64
-    static constexpr int bO = bQ + 2 * align_up(8 * NQ, 128);      // [8][..] update operand, FP64
+    static constexpr int NBUF = 3;                                // raw tiles in flight (this + 2 ahead)
+    static constexpr int bO = bQ + NBUF * align_up(8 * NQ, 128);   // [8][..] update operand, FP64
     static constexpr int bFc = bO + align_up(8 * NO, 128);         // [NLC][7] cell fluxes, FP64
     static constexpr int bP = bFc + align_up(8 * 7 * NLC, 16);     // [9][NLC] primitives, FP64
     static constexpr int bA = bP + align_up(8 * 9 * NLC, 16);      // [7][NLC] eigenvalues, R
@@ -129,7 +130,7 @@ struct Tile {
     static constexpr int lDecW = lCF + align_up(4 * 2 * NLC, 16);
     static constexpr int lEnd = lDecW + align_up(4 * NL * (F + 2), 16);
     static constexpr size_t bytes_learned = (size_t)lEnd;
-    static constexpr size_t bytes_plain = (size_t)bB + 3 * 8;
+    static constexpr size_t bytes_plain = (size_t)bB + (NBUF + 1) * 8;
     static constexpr size_t bytes_route = (size_t)bEnd;
     static constexpr uint32_t in_bytes = 8u * NQ;
     static constexpr uint32_t out_bytes = 8u * NO;
@@ -361,6 +362,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     using V2 = typename Math<R>::V2;
     constexpr int C = TL::C, F = TL::F, NP = TL::NP, NLC = TL::NLC, NLF = TL::NLF, NI = TL::NI;
     constexpr int TO = TL::TO;
+    constexpr int NBUF = TL::NBUF;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // TMA destinations need 128-byte alignment: align the carve-up base
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
@@ -466,9 +468,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     const bool issuer = tid == NT - 1;
 
     if (issuer) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        mbar_init(&bars[2], 1);
+        for (int k = 0; k <= NBUF; ++k) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
     __syncthreads();
@@ -503,8 +503,8 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             mbar_arrive_expect_tx(&bars[b], TL::in_bytes);
             tma_load_4d(sm + TL::bQ + b * align_up(8 * TL::NQ, 128), &a.tm_in, &bars[b], cc[0], cc[1], cc[2], cc[3]);
         } else {
-            mbar_arrive_expect_tx(&bars[2], TL::out_bytes);
-            tma_load_4d(sm + TL::bO, &a.tm_out, &bars[2], cc[0], cc[1], cc[2], cc[3]);
+            mbar_arrive_expect_tx(&bars[NBUF], TL::out_bytes);
+            tma_load_4d(sm + TL::bO, &a.tm_out, &bars[NBUF], cc[0], cc[1], cc[2], cc[3]);
         }
         return true;
     };
@@ -517,15 +517,23 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     uint32_t pend_bits = 0u;   // copies in flight per barrier (the issuer's view, bit k)
     bool issued_ok = true;
     if (issuer && tile < ntiles) {
+        // this tile's raw tile and update operand, and the raw tiles of the
+        // next NBUF - 1 tiles of this block
         issued_ok = issue(tile, 0, 0) && issue(tile, 1, 0);
-        pend_bits = issued_ok ? 5u : 0u;
+        pend_bits = issued_ok ? (1u | (1u << NBUF)) : 0u;
+        long long ahead = advance(tile + gridDim.x);
+        for (int k = 1; k < NBUF - 1 && ahead < ntiles; ++k) {
+            issued_ok = issue(ahead, 0, k) && issued_ok;
+            pend_bits |= 1u << k;
+            ahead = advance(ahead + gridDim.x);
+        }
     }
     // On a failed wait the whole block leaves together; the issuer first waits
     // (bounded) for the copies it still has in flight.
     auto bail = [&]() {
         if (issuer) {
             atomicOr(a0.status, HOW_STATUS_TMA_TIMEOUT);
-            for (int k = 0; k < 3; ++k)
+            for (int k = 0; k <= NBUF; ++k)
                 if ((pend_bits >> k) & 1u) mbar_wait_bounded(&bars[k], (par_bits >> k) & 1u, kWaitLimit);
         }
     };
@@ -584,10 +592,14 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         par_bits ^= 1u << buf;
         pend_bits &= ~(1u << buf);
         {
-            const long long next = advance(tile + gridDim.x);
-            if (issuer && next < ntiles) {
-                issued_ok = issue(next, 0, buf ^ 1) && issued_ok;
-                pend_bits |= 1u << (buf ^ 1);
+            // the raw tile NBUF - 1 tiles ahead, into the buffer the previous
+            // tile used (every read of it ended with that tile's last barrier)
+            long long ahead = advance(tile + gridDim.x);
+            for (int k = 2; k < NBUF; ++k) ahead = advance(ahead + gridDim.x);
+            const int nb = (buf + NBUF - 1) % NBUF;
+            if (issuer && ahead < ntiles) {
+                issued_ok = issue(ahead, 0, nb) && issued_ok;
+                pend_bits |= 1u << nb;
             }
         }
         // MODE 1: the routing pass's decisions for this tile's faces and one
@@ -1107,11 +1119,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
 
         // ------------------------------------------------------------ P5
         {
-            const bool ok = mbar_wait_bounded(&bars[2], (par_bits >> 2) & 1u, wait_limit);
+            const bool ok = mbar_wait_bounded(&bars[NBUF], (par_bits >> NBUF) & 1u, wait_limit);
             if (__syncthreads_or(!ok)) { bail(); return; }
         }
-        par_bits ^= 4u;
-        pend_bits &= ~4u;
+        par_bits ^= 1u << NBUF;
+        pend_bits &= ~(1u << NBUF);
         const double dtdl = dtdl_tile;
         for (int t = tid; t < 8 * NL * T; t += blockDim.x) {
             int v, l, ct;
@@ -1138,11 +1150,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             const long long next = advance(tile + gridDim.x);
             if (issuer && next < ntiles) {
                 issued_ok = issue(next, 1, 0) && issued_ok;
-                pend_bits |= 4u;
+                pend_bits |= 1u << NBUF;
             }
         }
         mark(10);
-        buf ^= 1;
+        buf = buf + 1 == NBUF ? 0 : buf + 1;
     }   // tile loop
 }
 
