@@ -652,5 +652,6 @@ int how_ensemble_member_status(const how_ensemble* e, int m, double* time, long*
 }
 
 long how_ensemble_graph_launches(const how_ensemble* e) { return e ? e->graph_launches : 0; }
+void* how_ensemble_stream(how_ensemble* e) { return e ? (void*)e->stream : nullptr; }
 
 }  // extern "C"

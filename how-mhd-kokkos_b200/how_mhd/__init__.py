@@ -131,6 +131,7 @@ def _load():
         "how_ensemble_member_status": ([V, ctypes.c_int, D, ctypes.POINTER(ctypes.c_long),
                                         ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "how_ensemble_graph_launches": ([V], ctypes.c_long),
+        "how_ensemble_stream": ([V], ctypes.c_void_p),
         "how_part_plan": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PartInfo)],
                           ctypes.c_int),
         "how_group_create": ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(V)], ctypes.c_int),
@@ -570,6 +571,11 @@ class Ensemble:
 
     def init(self):
         _check(_lib.how_ensemble_init(self._h))
+
+    @property
+    def stream(self):
+        """The ensemble's CUDA stream handle (cudaStream_t as an int)."""
+        return _lib.how_ensemble_stream(self._h)
 
     def set_shapes(self, sx, sy, sz=0):
         _check(_lib.how_ensemble_set_shapes(self._h, sx, sy, sz))

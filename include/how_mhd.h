@@ -252,6 +252,8 @@ int how_ensemble_shape_info(int dir, int shape, int* lines, int* cells);
 int how_ensemble_run(how_ensemble* e, long max_steps, long* steps_out);
 int how_ensemble_member_status(const how_ensemble* e, int m, double* time, long* steps, int* done);
 long how_ensemble_graph_launches(const how_ensemble* e);
+/* The ensemble's CUDA stream (cudaStream_t), for callers that time with events. */
+void* how_ensemble_stream(how_ensemble* e);
 
 /* ------------------------------------------------------- learned routing */
 /* No counterpart in the reference (an addition of this library).  A
