@@ -412,9 +412,13 @@ def bench_ours(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         barrier()
+        # an NVTX range around the timed steps, so a profiler can select
+        # their launches alone (ncu --nvtx --nvtx-include "timed_steps/")
+        torch.cuda.nvtx.range_push("timed_steps")
         e0.record(stream)
         dom.run(t_sim, args.steps)
         e1.record(stream)
+        torch.cuda.nvtx.range_pop()
         barrier()
         ms = e0.elapsed_time(e1)
         launches = dom.kernel_launches - l0

@@ -90,10 +90,11 @@ struct Tile {
     static constexpr int NO = 8 * NL * TO;          // update operand tile
     static constexpr int NS = 21;                   // eigen-system scalars per interface
     // byte offsets (base 128-byte aligned; TMA destinations on 128 B)
-    static constexpr int bQ = 0;                                   // 2 x [8][..] raw conserved, FP64
-    static constexpr int NBUF = 3;                                // raw tiles in flight (this + 2 ahead)
-    static constexpr int bO = bQ + NBUF * align_up(8 * NQ, 128);   // [8][..] update operand, FP64
-    static constexpr int bFc = bO + align_up(8 * NO, 128);         // [NLC][7] cell fluxes, FP64
+    static constexpr int bQ = 0;                                   // NBUF x [8][..] raw conserved, FP64
+    static constexpr int NBUF = 2;                                // raw tiles in flight (this + 1 ahead)
+    static constexpr int NOB = 2;                                 // update operands in flight (this + next)
+    static constexpr int bO = bQ + NBUF * align_up(8 * NQ, 128);   // NOB x [8][..] update operand, FP64
+    static constexpr int bFc = bO + NOB * align_up(8 * NO, 128);   // [NLC][7] cell fluxes, FP64
     static constexpr int bP = bFc + align_up(8 * 7 * NLC, 16);     // [9][NLC] primitives, FP64
     static constexpr int bA = bP + align_up(8 * 9 * NLC, 16);      // [7][NLC] eigenvalues, R
     static constexpr int bD = bA + align_up((int)sizeof(R) * 7 * NLC, 16);  // [NLC][14] dU, R
@@ -108,11 +109,12 @@ struct Tile {
     // left rows and right columns are rebuilt from them in registers where
     // they are used, never stored
     static constexpr int bS = bU + align_up(szU0 > szU1 ? szU0 : szU1, 16);
-    static constexpr int bB = bS + align_up((int)sizeof(R) * NS * NI, 16);   // 3 mbarriers
+    static constexpr int bB = bS + align_up((int)sizeof(R) * NS * NI, 16);   // NBUF + NOB mbarriers
+    static constexpr int szB = align_up(8 * (NBUF + NOB), 16);
     // routing (MODE 1-3): decision, compacted list, weight deviation and FP32
     // features of the tile's interfaces (collection), the linear flux's LF
     // speed, the cells' routing values (guard and collection)
-    static constexpr int bDec = bB + 32;                          // [NLF] int
+    static constexpr int bDec = bB + szB;                         // [NLF] int
     static constexpr int bList = bDec + align_up(4 * NLF, 16);    // [NLF] int
     static constexpr int bDev = bList + align_up(4 * NLF, 16);    // [NLF] float (bits)
     static constexpr int bFlx = bDev + align_up(4 * NLF, 16);     // [NLF] float (bits): flux departure
@@ -123,14 +125,15 @@ struct Tile {
     static constexpr int bEnd = bDecW + align_up(4 * NL * (F + 2), 16);
     // learned routing (MODE 1) keeps only what it uses: decisions, list, LF
     // speed, the cells' density and pressure (the guard), fetched decisions
-    static constexpr int lDec = bB + 32;
+    // (two sets: this tile's and the next tile's)
+    static constexpr int lDec = bB + szB;
     static constexpr int lList = lDec + align_up(4 * NLF, 16);
     static constexpr int lAmx = lList + align_up(4 * NLF, 16);
     static constexpr int lCF = lAmx + align_up((int)sizeof(R) * NLF, 16);
     static constexpr int lDecW = lCF + align_up(4 * 2 * NLC, 16);
-    static constexpr int lEnd = lDecW + align_up(4 * NL * (F + 2), 16);
+    static constexpr int lEnd = lDecW + 2 * align_up(4 * NL * (F + 2), 16);
     static constexpr size_t bytes_learned = (size_t)lEnd;
-    static constexpr size_t bytes_plain = (size_t)bB + (NBUF + 1) * 8;
+    static constexpr size_t bytes_plain = (size_t)bB + (NBUF + NOB) * 8;
     static constexpr size_t bytes_route = (size_t)bEnd;
     static constexpr uint32_t in_bytes = 8u * NQ;
     static constexpr uint32_t out_bytes = 8u * NO;
@@ -362,7 +365,9 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     using V2 = typename Math<R>::V2;
     constexpr int C = TL::C, F = TL::F, NP = TL::NP, NLC = TL::NLC, NLF = TL::NLF, NI = TL::NI;
     constexpr int TO = TL::TO;
-    constexpr int NBUF = TL::NBUF;
+    constexpr int NBUF = TL::NBUF, NOB = TL::NOB;
+    constexpr int FE = F + 2;                                  // fetched decisions per line (MODE 1)
+    constexpr int DWS = align_up(4 * NL * FE, 16) / 4;         // ints per decision set
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // TMA destinations need 128-byte alignment: align the carve-up base
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
@@ -468,13 +473,13 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
     const bool issuer = tid == NT - 1;
 
     if (issuer) {
-        for (int k = 0; k <= NBUF; ++k) mbar_init(&bars[k], 1);
+        for (int k = 0; k < NBUF + NOB; ++k) mbar_init(&bars[k], 1);
         fence_barrier_init();
     }
     __syncthreads();
 
-    // TMA loads (the issuer only): the raw tile of `tile` into buffer b
-    // (which == 0) or its update operand (which == 1).
+    // TMA loads (the issuer only): the raw tile of `tile` into raw buffer b
+    // (which == 0) or its update operand into operand buffer b (which == 1).
     auto issue = [&](long long gtile, int which, int b) -> bool {
         long long tile;
         const SweepArgs& a = *args_of(gtile, tile);
@@ -503,16 +508,45 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             mbar_arrive_expect_tx(&bars[b], TL::in_bytes);
             tma_load_4d(sm + TL::bQ + b * align_up(8 * TL::NQ, 128), &a.tm_in, &bars[b], cc[0], cc[1], cc[2], cc[3]);
         } else {
-            mbar_arrive_expect_tx(&bars[NBUF], TL::out_bytes);
-            tma_load_4d(sm + TL::bO, &a.tm_out, &bars[NBUF], cc[0], cc[1], cc[2], cc[3]);
+            mbar_arrive_expect_tx(&bars[NBUF + b], TL::out_bytes);
+            tma_load_4d(sm + TL::bO + b * align_up(8 * TL::NO, 128), &a.tm_out, &bars[NBUF + b], cc[0], cc[1], cc[2],
+                        cc[3]);
         }
         return true;
+    };
+    // MODE 1: the routing pass's decisions for tile t's faces and one more on
+    // each side of every line (faces -1 .. F), fetched by asynchronous 4-byte
+    // copies of the aligned words that hold them into decision set `slot`,
+    // one tile ahead so their latency hides behind a whole tile.  Every
+    // thread commits one group per call (empty past the last tile); returns
+    // the byte of this thread's word, -1 for no face.
+    auto fetch_dec = [&](long long t, int slot) -> int {
+        int shift = -1;
+        if constexpr (MODE == 1) {
+            static_assert(NL * FE <= NT, "one fetched decision per thread");
+            if (tid < NL * FE && t < ntiles) {
+                const Geo G = geo_of(a0.g);
+                int tx, ty, tz;
+                tile_coords(t, G.ntx, G.nty, tx, ty, tz);
+                const int l = tid / FE, f = tid % FE - 1;
+                const int t1 = line0 + ty * NL + l, iface = tx * T + f;
+                if (t1 >= 3 && t1 <= G.nt1 + 2 && iface >= 0 && iface <= G.n) {
+                    const unsigned char* src = a0.route_next + route_line(a0.g, DIR, t1, 3 + tz) + (iface + 2);
+                    shift = (int)(reinterpret_cast<uintptr_t>(src) & 3u);
+                    cp_async4(&sDecW[slot * DWS + tid],
+                              reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3)));
+                }
+            }
+            cp_async_commit();
+        }
+        return shift;
     };
 
     // a single domain's dt / d is one value for the whole launch
     const double dtdl_launch = ENS ? 0.0 : *a0.dtdl;
     long long tile = advance(blockIdx.x);
-    int buf = 0;
+    int buf = 0;               // raw buffer of this tile
+    int ob = 0;                // update operand buffer and decision set of this tile
     uint32_t par_bits = 0u;    // phase parity per barrier (bit k)
     uint32_t pend_bits = 0u;   // copies in flight per barrier (the issuer's view, bit k)
     bool issued_ok = true;
@@ -528,12 +562,13 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             ahead = advance(ahead + gridDim.x);
         }
     }
+    int dec_cur = fetch_dec(tile, 0);   // this tile's decision words (MODE 1)
     // On a failed wait the whole block leaves together; the issuer first waits
     // (bounded) for the copies it still has in flight.
     auto bail = [&]() {
         if (issuer) {
             atomicOr(a0.status, HOW_STATUS_TMA_TIMEOUT);
-            for (int k = 0; k <= NBUF; ++k)
+            for (int k = 0; k < NBUF + NOB; ++k)
                 if ((pend_bits >> k) & 1u) mbar_wait_bounded(&bars[k], (par_bits >> k) & 1u, kWaitLimit);
         }
     };
@@ -573,7 +608,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         // the line's first byte in the router's per-face arrays (route_line)
         auto rline = [&](int l) -> long long { return route_line(g, DIR, t1_0 + l, t2); };
         const double* sQ = reinterpret_cast<const double*>(sm + TL::bQ + buf * align_up(8 * TL::NQ, 128));
-        const double* sO = reinterpret_cast<const double*>(sm + TL::bO);
+        const double* sO = reinterpret_cast<const double*>(sm + TL::bO + ob * align_up(8 * TL::NO, 128));
         // raw conserved of line variable v at (line l, tile cell c); box order
         // x: [var][line][cell], y/z: [var][cell][line]
         auto qraw = [&](int v, int l, int c) -> double {
@@ -591,36 +626,25 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
         }
         par_bits ^= 1u << buf;
         pend_bits &= ~(1u << buf);
+        const long long next = advance(tile + gridDim.x);
         {
             // the raw tile NBUF - 1 tiles ahead, into the buffer the previous
-            // tile used (every read of it ended with that tile's last barrier)
-            long long ahead = advance(tile + gridDim.x);
+            // tile used, and the next tile's update operand into the operand
+            // buffer the previous tile used (every read of both ended with
+            // that tile's last barrier)
+            long long ahead = next;
             for (int k = 2; k < NBUF; ++k) ahead = advance(ahead + gridDim.x);
             const int nb = (buf + NBUF - 1) % NBUF;
             if (issuer && ahead < ntiles) {
                 issued_ok = issue(ahead, 0, nb) && issued_ok;
                 pend_bits |= 1u << nb;
             }
-        }
-        // MODE 1: the routing pass's decisions for this tile's faces and one
-        // more on each side of every line (faces -1 .. F), fetched now by
-        // asynchronous 4-byte copies of the aligned words that hold them, so
-        // their latency hides behind P1
-        constexpr int FE = F + 2;
-        int dec_shift = -1;   // byte of the word, -1: no face
-        if constexpr (MODE == 1) {
-            static_assert(NL * FE <= NT, "one fetched decision per thread");
-            if (tid < NL * FE) {
-                const int l = tid / FE, f = tid % FE - 1;
-                const int iface = c0 + f;
-                if (line_ok(l) && iface >= 0 && iface <= n) {
-                    const unsigned char* src = a.route_next + rline(l) + (iface + 2);
-                    dec_shift = (int)(reinterpret_cast<uintptr_t>(src) & 3u);
-                    cp_async4(&sDecW[tid], reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3)));
-                }
+            if (issuer && next < ntiles) {
+                issued_ok = issue(next, 1, ob ^ 1) && issued_ok;
+                pend_bits |= 1u << (NBUF + (ob ^ 1));
             }
-            cp_async_commit();
         }
+        const int dec_next = fetch_dec(next, ob ^ 1);   // the next tile's decisions (MODE 1)
         // this stage's dt / d (per member in an ensemble), used in P5
         const double dtdl_tile = ENS ? *a.dtdl : dtdl_launch;
         mark(0);
@@ -775,10 +799,13 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             if (tid == 0) s_nfull = 0;
         }
         if constexpr (MODE == 1) {
-            // the fetched decision words have arrived: keep this thread's byte
-            cp_async_wait_all();
-            if (tid < NL * FE)
-                sDecW[tid] = dec_shift < 0 ? 0 : (int)((((unsigned int)sDecW[tid]) >> (8 * dec_shift)) & 0xffu);
+            // this tile's decision words (fetched one tile ago) have arrived:
+            // keep this thread's byte
+            cp_async_wait_prior();
+            if (tid < NL * FE) {
+                int* w = sDecW + ob * DWS + tid;
+                *w = dec_cur < 0 ? 0 : (int)((((unsigned int)*w) >> (8 * dec_cur)) & 0xffu);
+            }
         }
         __syncthreads();
         mark(2);
@@ -821,7 +848,7 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
                 bool owned = false, full = false;
                 if (tid < NLF) {
                     const int l = tid / F, f = tid % F;
-                    const int* d = sDecW + l * FE + f;   // faces f-1, f, f+1
+                    const int* d = sDecW + ob * DWS + l * FE + f;   // faces f-1, f, f+1
                     // the hard guard on this stage's state, whatever the stage
                     // the network's decisions were formed at
                     const bool guard = router_guard_rp(sCF + l * C + f, sCF + NLC + l * C + f, (float)a.rhomin,
@@ -1119,11 +1146,11 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
 
         // ------------------------------------------------------------ P5
         {
-            const bool ok = mbar_wait_bounded(&bars[NBUF], (par_bits >> NBUF) & 1u, wait_limit);
+            const bool ok = mbar_wait_bounded(&bars[NBUF + ob], (par_bits >> (NBUF + ob)) & 1u, wait_limit);
             if (__syncthreads_or(!ok)) { bail(); return; }
         }
-        par_bits ^= 1u << NBUF;
-        pend_bits &= ~(1u << NBUF);
+        par_bits ^= 1u << (NBUF + ob);
+        pend_bits &= ~(1u << (NBUF + ob));
         const double dtdl = dtdl_tile;
         for (int t = tid; t < 8 * NL * T; t += blockDim.x) {
             int v, l, ct;
@@ -1146,15 +1173,10 @@ __global__ void __launch_bounds__(NT, MINB) k_sweep(const __grid_constant__ Swee
             }
         }
         __syncthreads();   // every read of the update operand / raw tile is done
-        {
-            const long long next = advance(tile + gridDim.x);
-            if (issuer && next < ntiles) {
-                issued_ok = issue(next, 1, 0) && issued_ok;
-                pend_bits |= 1u << NBUF;
-            }
-        }
         mark(10);
         buf = buf + 1 == NBUF ? 0 : buf + 1;
+        ob ^= 1;
+        dec_cur = dec_next;
     }   // tile loop
 }
 
