@@ -423,6 +423,20 @@ int how_group_get_state(how_group* g, double* q) {
     return HOW_OK;
 }
 
+int how_group_output(how_group* g, int step, double time, const char* dir) {
+    if (!g) { set_error("null group"); return HOW_ERR_ARG; }
+    // every part writes its piece, named and headed as the reference's MPI
+    // rank of the same slab writes it (src/output.cpp:21-38, 85-91, 383-402)
+    for (int p = 0; p < g->n; ++p) {
+        int rc = set_dev(g, p);
+        if (!rc) rc = how_output(g->parts[p], step, time, dir);
+        if (rc) return rc;
+    }
+    const std::string fmt = g->global.output_format;
+    if (fmt != "vts" && fmt != "vtk") return HOW_OK;
+    return write_pvts(g->global, g->n, g->kstart.data(), g->nzl.data(), step, dir);
+}
+
 int how_group_get_face_b(how_group* g, double* bx, double* by, double* bz) {
     if (!g || !bx || !by || !bz) { set_error("null argument"); return HOW_ERR_ARG; }
     const how_params& gp = g->global;

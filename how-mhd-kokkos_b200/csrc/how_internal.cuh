@@ -202,6 +202,8 @@ void launch_fluxct(Ctx& c, int iw, double k1, double k3);
 // each ending with the local fills of the arrays part_halo_fields names
 void launch_ct_part(Ctx& c, int seg, int iw, double k1, double k3, double c4, double c5, int stage5);
 int part_halo_fields(Ctx& c, int seg, int iw, double** out);
+// the .pvts master file of a z-decomposed domain's .vts pieces (output.cu)
+int write_pvts(const how_params& gp, int nparts, const int* kstart, const int* nzl, int step, const char* dir);
 // the sweeps of stage iw (with the stage-5 base), before its CT (capi.cu)
 void stage_sweeps(Ctx& c, int iw);
 // CFL reduction of stage 0 into the device maxima, and dt from them

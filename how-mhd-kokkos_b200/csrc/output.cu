@@ -56,6 +56,7 @@ struct DumpArgs {
     const double* q;          // q(0), device layout
     double* out;              // slab payload (staging buffer)
     int k0, nk;               // slab: padded planes k0 .. k0 + nk - 1
+    int kofs;                 // global index of the first active plane (a part's kstart)
     int px, py, pz;           // periodic axes
     double dx, dy, dz, gam;
 };
@@ -71,7 +72,7 @@ __device__ __forceinline__ DumpCell dump_cell(const DumpArgs& a, int i, int j, i
     DumpCell d;
     d.x = __dmul_rn(__dadd_rn((double)(i - 3), 0.5), a.dx);
     d.y = __dmul_rn(__dadd_rn((double)(j - 3), 0.5), a.dy);
-    d.z = __dmul_rn(__dadd_rn((double)(k - 3), 0.5), a.dz);
+    d.z = __dmul_rn(__dadd_rn((double)(a.kofs + k - 3), 0.5), a.dz);
     d.rho = a.q[c];
     d.Mx = a.q[fs + c]; d.My = a.q[2 * fs + c]; d.Mz = a.q[3 * fs + c];
     d.Bx = a.q[4 * fs + c]; d.By = a.q[5 * fs + c]; d.Bz = a.q[6 * fs + c];
@@ -177,12 +178,19 @@ bool pwrite_all(int fd, const void* data, size_t n, off_t off) {
     return true;
 }
 
-// make_output_filename (src/output.cpp:21-38), serial form: <dir>/dumpNNNNNN<ext>
-std::string dump_name(const char* dir, int step, const char* ext) {
-    char b[32];
-    std::snprintf(b, sizeof(b), "dump%06d%s", step, ext);
+// make_output_filename (src/output.cpp:21-38): <dir>/dumpNNNNNN<ext>, or for
+// one part of a decomposed domain, the MPI form <dir>/dumpNNNNNN_rankRRRRRR<ext>
+std::string dump_file(int step, const char* ext, int rank) {
+    char b[48];
+    if (rank >= 0) std::snprintf(b, sizeof(b), "dump%06d_rank%06d%s", step, rank, ext);
+    else std::snprintf(b, sizeof(b), "dump%06d%s", step, ext);
+    return b;
+}
+
+std::string dump_name(const char* dir, int step, const char* ext, int rank) {
+    const std::string b = dump_file(step, ext, rank);
     std::string d = dir ? dir : "output";
-    return d.empty() ? std::string(b) : d + "/" + b;
+    return d.empty() ? b : d + "/" + b;
 }
 
 int make_dirs(const std::string& dir) {
@@ -218,6 +226,7 @@ DumpArgs dump_args(const Ctx& c) {
     a.q = c.q[0];
     a.out = c.stage_buf;
     a.k0 = 3; a.nk = 0;
+    a.kofs = c.part >= 0 ? c.kstart : 0;
     a.px = c.p.bc[0] == HOW_BC_PERIODIC;
     a.py = c.p.bc[1] == HOW_BC_PERIODIC;
     a.pz = c.p.bc[2] == HOW_BC_PERIODIC;
@@ -225,11 +234,27 @@ DumpArgs dump_args(const Ctx& c) {
     return a;
 }
 
+// Where a file's cells sit in the whole domain: the header fields the
+// reference fills from its MPI decomposition (cart_rank, gnx/gny/gnz,
+// istart/jstart/kstart, src/parameters.hpp:20, 59, 71).  A single domain is
+// rank 0 at the origin; a part of a z-decomposed group is rank `part` (the
+// Cartesian rank of a 1 x 1 x P layout) starting at global plane kstart.
+struct PieceInfo {
+    int rank, gnx, gny, gnz, istart, jstart, kstart;
+};
+
+PieceInfo piece_of(const Ctx& c) {
+    PieceInfo pi{0, c.g.nx, c.g.ny, c.g.nz, 0, 0, 0};
+    if (c.part >= 0) { pi.rank = c.part; pi.gnz = c.gnz; pi.kstart = c.kstart; }
+    return pi;
+}
+
 // Supplies the payload of active planes [k0, k0 + nk) in the kernels' slab
 // layout, host-resident.
 using SlabFn = std::function<int(int k0, int nk, const double** data)>;
 
-int assemble_vts(const Grid& g, int step, double time, const std::string& path, int K, const SlabFn& slab) {
+int assemble_vts(const Grid& g, const PieceInfo& pi, int step, double time, const std::string& path, int K,
+                 const SlabFn& slab) {
     const long long npts = (long long)g.nx * g.ny * g.nz;
     // appended blocks: [u64 bytes][payload], offsets from the byte after "_"
     const int ncomp[10] = {1, 1, 1, 1, 1, 1, 3, 3, 3, 3};
@@ -240,10 +265,11 @@ int assemble_vts(const Grid& g, int step, double time, const std::string& path, 
     std::string h;
     h += "<?xml version=\"1.0\"?>\n";
     h += "<VTKFile type=\"StructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" header_type=\"UInt64\">\n";
-    h += "  <StructuredGrid WholeExtent=\"0 "; put_int(h, g.nx - 1); h += " 0 "; put_int(h, g.ny - 1);
-    h += " 0 "; put_int(h, g.nz - 1); h += "\">\n";
-    h += "    <Piece Extent=\"0 "; put_int(h, g.nx - 1); h += " 0 "; put_int(h, g.ny - 1);
-    h += " 0 "; put_int(h, g.nz - 1); h += "\">\n";
+    h += "  <StructuredGrid WholeExtent=\"0 "; put_int(h, pi.gnx - 1); h += " 0 "; put_int(h, pi.gny - 1);
+    h += " 0 "; put_int(h, pi.gnz - 1); h += "\">\n";
+    h += "    <Piece Extent=\""; put_int(h, pi.istart); h += " "; put_int(h, pi.istart + g.nx - 1);
+    h += " "; put_int(h, pi.jstart); h += " "; put_int(h, pi.jstart + g.ny - 1);
+    h += " "; put_int(h, pi.kstart); h += " "; put_int(h, pi.kstart + g.nz - 1); h += "\">\n";
     h += "      <FieldData>\n";
     h += "        <DataArray type=\"Float64\" Name=\"time\" NumberOfTuples=\"1\" format=\"ascii\">\n";
     h += "          "; put_sci(h, time); h += "\n";
@@ -252,11 +278,12 @@ int assemble_vts(const Grid& g, int step, double time, const std::string& path, 
     h += "          "; put_int(h, step); h += "\n";
     h += "        </DataArray>\n";
     h += "        <DataArray type=\"Int32\" Name=\"rank\" NumberOfTuples=\"1\" format=\"ascii\">\n";
-    h += "          0\n";
+    h += "          "; put_int(h, pi.rank); h += "\n";
     h += "        </DataArray>\n";
     h += "        <DataArray type=\"Int32\" Name=\"global_start_index\" NumberOfComponents=\"3\" "
          "NumberOfTuples=\"1\" format=\"ascii\">\n";
-    h += "          0 0 0\n";
+    h += "          "; put_int(h, pi.istart); h += " "; put_int(h, pi.jstart); h += " "; put_int(h, pi.kstart);
+    h += "\n";
     h += "        </DataArray>\n";
     h += "      </FieldData>\n";
     h += "      <PointData>\n";
@@ -309,17 +336,19 @@ int assemble_vts(const Grid& g, int step, double time, const std::string& path, 
     return HOW_OK;
 }
 
-int assemble_dat(const Grid& g, int step, double time, const std::string& path, int K, const SlabFn& slab) {
+int assemble_dat(const Grid& g, const PieceInfo& pi, int step, double time, const std::string& path, int K,
+                 const SlabFn& slab) {
     std::FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) { set_error("cannot open output file %s: %s", path.c_str(), std::strerror(errno)); return HOW_ERR_ARG; }
     std::string h;
     h += "# step = "; put_int(h, step); h += "\n";
     h += "# time = "; put_sci(h, time); h += "\n";
-    h += "# rank = 0\n";
+    h += "# rank = "; put_int(h, pi.rank); h += "\n";
     h += "# local_active_size = "; put_int(h, g.nx); h += " "; put_int(h, g.ny); h += " "; put_int(h, g.nz); h += "\n";
-    h += "# global_active_size = "; put_int(h, g.nx); h += " "; put_int(h, g.ny); h += " "; put_int(h, g.nz);
+    h += "# global_active_size = "; put_int(h, pi.gnx); h += " "; put_int(h, pi.gny); h += " "; put_int(h, pi.gnz);
     h += "\n";
-    h += "# global_start_index = 0 0 0\n";
+    h += "# global_start_index = "; put_int(h, pi.istart); h += " "; put_int(h, pi.jstart); h += " ";
+    put_int(h, pi.kstart); h += "\n";
     h += "# columns: ig jg kg il jl kl x y z rho Mx My Mz Bx By Bz E pg vx vy vz divB\n";
     bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
     int rc = HOW_OK;
@@ -338,7 +367,8 @@ int assemble_dat(const Grid& g, int step, double time, const std::string& path, 
             s.reserve((size_t)g.nx * 400);
             for (int il = 0; il < g.nx; ++il) {
                 const double* v = src + kDatCols * ((long long)r * g.nx + il);
-                put_int(s, il); s += ' '; put_int(s, jl); s += ' '; put_int(s, kl); s += ' ';
+                put_int(s, pi.istart + il); s += ' '; put_int(s, pi.jstart + jl); s += ' ';
+                put_int(s, pi.kstart + kl); s += ' ';
                 put_int(s, il); s += ' '; put_int(s, jl); s += ' '; put_int(s, kl);
                 for (int m = 0; m < kDatCols; ++m) { s += ' '; put_sci(s, v[m]); }
                 s += '\n';
@@ -374,7 +404,7 @@ int dump_prologue(how_ctx* c, const char* dir, bool* dat, bool* skip, std::strin
     }
     const int rc = make_dirs(dir ? dir : "output");
     if (rc) return rc;
-    *path = dump_name(dir, step, *dat ? ".dat" : ".vts");
+    *path = dump_name(dir, step, *dat ? ".dat" : ".vts", c->part);
     return HOW_OK;
 }
 
@@ -418,6 +448,46 @@ void dump_release(Ctx& c) {
     c.dump = nullptr;
 }
 
+// The master file of a decomposed domain's .vts pieces: a VTK XML
+// PStructuredGrid over the whole extent, declaring the pieces' arrays and
+// listing each piece's extent and file (relative to the master's directory).
+// The reference lists this file as a to-do (README.md:758): its MPI ranks
+// write only their pieces.  As there, a piece's points are its own cell
+// centres, so neighbouring pieces do not share a layer of points.
+int write_pvts(const how_params& gp, int nparts, const int* kstart, const int* nzl, int step, const char* dir) {
+    std::string h;
+    h += "<?xml version=\"1.0\"?>\n";
+    h += "<VTKFile type=\"PStructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" header_type=\"UInt64\">\n";
+    h += "  <PStructuredGrid WholeExtent=\"0 "; put_int(h, gp.nx - 1); h += " 0 "; put_int(h, gp.ny - 1);
+    h += " 0 "; put_int(h, gp.nz - 1); h += "\" GhostLevel=\"0\">\n";
+    h += "    <PPointData>\n";
+    const char* names[9] = {"rho", "pressure", "energy", "v2", "B2", "divB", "velocity", "magnetic_field",
+                            "momentum"};
+    for (int b = 0; b < 9; ++b) {
+        h += "      <PDataArray type=\"Float64\" Name=\""; h += names[b];
+        h += "\" NumberOfComponents=\""; put_int(h, b < 6 ? 1 : 3); h += "\"/>\n";
+    }
+    h += "    </PPointData>\n";
+    h += "    <PCellData>\n";
+    h += "    </PCellData>\n";
+    h += "    <PPoints>\n";
+    h += "      <PDataArray type=\"Float64\" NumberOfComponents=\"3\"/>\n";
+    h += "    </PPoints>\n";
+    for (int p = 0; p < nparts; ++p) {
+        h += "    <Piece Extent=\"0 "; put_int(h, gp.nx - 1); h += " 0 "; put_int(h, gp.ny - 1);
+        h += " "; put_int(h, kstart[p]); h += " "; put_int(h, kstart[p] + nzl[p] - 1);
+        h += "\" Source=\""; h += dump_file(step, ".vts", p); h += "\"/>\n";
+    }
+    h += "  </PStructuredGrid>\n";
+    h += "</VTKFile>\n";
+    const std::string path = dump_name(dir, step, ".pvts", -1);
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) { set_error("cannot open output file %s: %s", path.c_str(), std::strerror(errno)); return HOW_ERR_ARG; }
+    const bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
+    if (std::fclose(f) != 0 || !ok) { set_error("write to %s failed", path.c_str()); return HOW_ERR_ARG; }
+    return HOW_OK;
+}
+
 }  // namespace how
 
 using namespace how;
@@ -445,7 +515,9 @@ extern "C" int how_output(how_ctx* c, int step, double time, const char* dir) {
         *data = host.data();
         return HOW_OK;
     };
-    return dat ? assemble_dat(c->g, step, time, path, K, slab) : assemble_vts(c->g, step, time, path, K, slab);
+    const PieceInfo pi = piece_of(*c);
+    return dat ? assemble_dat(c->g, pi, step, time, path, K, slab)
+               : assemble_vts(c->g, pi, step, time, path, K, slab);
 }
 
 extern "C" int how_output_async(how_ctx* c, int step, double time, const char* dir) {
@@ -488,7 +560,8 @@ extern "C" int how_output_async(how_ctx* c, int step, double time, const char* d
     j->err.clear();
     const int dev = c->dev;
     const Grid gg = g;
-    j->writer = std::thread([j, dev, gg, step, time, path, dat]() {
+    const PieceInfo pi = piece_of(*c);
+    j->writer = std::thread([j, dev, gg, pi, step, time, path, dat]() {
         int r = HOW_OK;
         cudaError_t e = cudaSetDevice(dev);
         if (e == cudaSuccess) e = cudaEventSynchronize(j->copied);
@@ -497,7 +570,8 @@ extern "C" int how_output_async(how_ctx* c, int step, double time, const char* d
         } else {
             const double* host = j->host;
             SlabFn whole = [host](int, int, const double** data) -> int { *data = host; return HOW_OK; };
-            r = dat ? assemble_dat(gg, step, time, path, gg.nz, whole) : assemble_vts(gg, step, time, path, gg.nz, whole);
+            r = dat ? assemble_dat(gg, pi, step, time, path, gg.nz, whole)
+                    : assemble_vts(gg, pi, step, time, path, gg.nz, whole);
         }
         j->rc = r;
         if (r) j->err = how_last_error();

@@ -145,6 +145,7 @@ def _load():
         "how_group_run": ([V, D, ctypes.c_long, ctypes.POINTER(ctypes.c_long), D, ctypes.c_long], ctypes.c_int),
         "how_group_get_state": ([V, D], ctypes.c_int),
         "how_group_get_face_b": ([V, D, D, D], ctypes.c_int),
+        "how_group_output": ([V, ctypes.c_int, ctypes.c_double, ctypes.c_char_p], ctypes.c_int),
         "how_router_param_count": ([], ctypes.c_int),
         "how_router_default": ([F, ctypes.c_int, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
         "how_router_set_weights": ([V, F, ctypes.c_int], ctypes.c_int),
@@ -271,11 +272,13 @@ class Domain:
         self.shape = p.shape
 
     @classmethod
-    def _borrowed(cls, handle, owner):
-        """A view of a context owned by someone else (an ensemble member)."""
+    def _borrowed(cls, handle, owner, part=None):
+        """A view of a context owned by someone else (an ensemble member, or
+        part `part` of a decomposed group)."""
         d = cls.__new__(cls)
         d._h = ctypes.c_void_p(handle)
         d._owner = owner
+        d._part = part
         p = Params()
         _check(_lib.how_get_params(d._h, ctypes.byref(p)))
         d.params = p
@@ -379,7 +382,8 @@ class Domain:
             else str(self.params.output_format)
         if fmt == "none":
             return None
-        name = "dump%06d%s" % (int(step), ".dat" if fmt == "dat" else ".vts")
+        rank = "" if getattr(self, "_part", None) is None else "_rank%06d" % self._part
+        name = "dump%06d%s%s" % (int(step), rank, ".dat" if fmt == "dat" else ".vts")
         return name if d == "" else d + "/" + name
 
     def output(self, step, time, directory=None):
@@ -488,7 +492,7 @@ class Group:
         self.params = params
         self.n = nparts
         self.shape = params.shape
-        self.parts = [Domain._borrowed(_lib.how_group_part(h, k), self) for k in range(nparts)]
+        self.parts = [Domain._borrowed(_lib.how_group_part(h, k), self, part=k) for k in range(nparts)]
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -538,6 +542,22 @@ class Group:
         b = [np.zeros(self.shape) for _ in range(3)]
         _check(_lib.how_group_get_face_b(self._h, *(_dptr(x) for x in b)))
         return b
+
+    def output(self, step, time, directory=None):
+        """Every part's dump piece, as the reference's MPI rank of the same
+        slab writes it (<directory>/dumpNNNNNN_rankPPPPPP.dat or .vts), and for
+        .vts the PStructuredGrid master <directory>/dumpNNNNNN.pvts.  Returns
+        (master path or None, [piece paths]); (None, []) for output_format none."""
+        d = "output" if directory is None else str(directory)
+        _check(_lib.how_group_output(self._h, int(step), float(time), d.encode()))
+        pieces = [p._dump_path(step, d) for p in self.parts]
+        if pieces[0] is None:
+            return None, []
+        master = None
+        if pieces[0].endswith(".vts"):
+            name = "dump%06d.pvts" % int(step)
+            master = name if d == "" else d + "/" + name
+        return master, pieces
 
 
 class Ensemble:

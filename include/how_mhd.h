@@ -342,6 +342,17 @@ int how_group_run(how_group* g, double* time, long max_steps, long* steps, doubl
 /* active cells of stage 0 / face B gathered into global reference-layout arrays */
 int how_group_get_state(how_group* g, double* q_global);
 int how_group_get_face_b(how_group* g, double* bx, double* by, double* bz);
+/* output(q, par, step, time) of every MPI rank (src/output.cpp:555-572) for
+ * the parts: part p writes <dir>/dumpNNNNNN_rankPPPPPP.dat|.vts, the piece
+ * the reference's rank p of a 1 x 1 x nparts layout writes, with the same
+ * header fields (rank, global and local sizes, global start index, piece
+ * extent), global indices and coordinates, and the divB diagnostic over the
+ * piece's own cells (wrapped or clamped at the piece's edges, as the
+ * reference's per-rank writer does).  For vts/vtk it also writes
+ * <dir>/dumpNNNNNN.pvts, the PStructuredGrid master file that lists the pieces
+ * (a to-do of the reference, README.md:758).  how_output on a part's context
+ * (how_group_part) writes that part's piece alone.  "none" writes nothing. */
+int how_group_output(how_group* g, int step, double time, const char* dir);
 
 /* ---------------------------------------------------- allocation-free use */
 /* Capacity of the fixed scratch behind how_tstep_noalloc, in (i, j) lines. */

@@ -27,6 +27,14 @@
 //                  (src/output.cpp:555-572) on the initial or --state q(0):
 //                  output/dumpSSSSSS.dat or .vts in the working directory, in
 //                  the input's output_format.  <out.bin> is not written.
+//   --piece R NZ KS : with --output, write what MPI rank R of a z-split
+//                  writes for its slab: after setup_mpi_domain the local
+//                  sizes and offsets its decomposition would set (nz = NZ,
+//                  kstart = KS, cart_rank = R; gnz, dz stay the input's), so
+//                  --state holds the slab (nx+6, ny+6, NZ+6).  The serial
+//                  build names the file without the _rank suffix; its bytes
+//                  are the MPI rank's (src/output.cpp:21-38 is the only
+//                  USE_MPI difference in the writer).
 //
 // Dump format: a sequence of records
 //   u32 name_len, name bytes, u32 ndim, u64 dims[ndim], f64 data[prod(dims)]
@@ -187,6 +195,7 @@ int main(int argc, char** argv) {
     std::string state_path, sweep;
     double sweep_dt = 0.0;
     bool dump_stages = false, time_only = false, do_output = false;
+    int piece_rank = -1, piece_nz = 0, piece_kstart = 0;
     int out_step = 0;
     double out_time = 0.0;
     for (int a = 3; a < argc; ++a) {
@@ -199,6 +208,11 @@ int main(int argc, char** argv) {
         else if (s == "--threads" && a + 1 < argc) omp_set_num_threads(std::atoi(argv[++a]));
         else if (s == "--time-only") time_only = true;
         else if (s == "--warmup" && a + 1 < argc) warmup = std::atol(argv[++a]);
+        else if (s == "--piece" && a + 3 < argc) {
+            piece_rank = std::atoi(argv[++a]);
+            piece_nz = std::atoi(argv[++a]);
+            piece_kstart = std::atoi(argv[++a]);
+        }
         else if (s == "--output" && a + 2 < argc) {
             do_output = true;
             out_step = std::atoi(argv[++a]);
@@ -217,6 +231,11 @@ int main(int argc, char** argv) {
         read_parameters(in, par);
         finalize_parameters_after_read(par);
         setup_mpi_domain(par);
+        if (piece_rank >= 0) {
+            par.nz = piece_nz;
+            par.kstart = piece_kstart;
+            par.cart_rank = piece_rank;
+        }
 
         // src/main.cpp:114-120
         Kokkos::View<double*****> q("q", 6, 8, par.nx + 6, par.ny + 6, par.nz + 6);

@@ -145,3 +145,60 @@ def test_driver_writes_the_reference_dumps(tmp_path):
     subprocess.run([str(REF_BIN), str(inp), "/dev/null", "--output", "0", "0.0"], cwd=tmp_path, check=True,
                    capture_output=True, timeout=300)
     assert (run / "output" / "dump000000.vts").read_bytes() == (tmp_path / "output" / "dump000000.vts").read_bytes()
+
+
+GROUP_CASES = [
+    # (problem, grid, boundaries, parts)
+    ("mpi_smooth3d", (12, 10, 9), ("periodic", "open", "periodic"), 3),
+    ("blast3d_b", (16, 12, 14), ("periodic", "periodic", "open"), 2),
+]
+
+
+@pytest.mark.parametrize("fmt", ["vts", "dat"])
+@pytest.mark.parametrize("case", GROUP_CASES, ids=[c[0] for c in GROUP_CASES])
+def test_group_pieces_are_the_reference_ranks_files(tmp_path, case, fmt):
+    """A z-decomposed group writes one piece per part, and each piece is the
+    file the reference's MPI rank of that slab writes (its own output() run on
+    the slab with the rank's nz, kstart and cart_rank), byte for byte:
+    header fields, global indices and coordinates, and the divB diagnostic
+    wrapped or clamped at the slab's own edges.  For .vts a PStructuredGrid
+    master lists the pieces with extents that tile the whole extent."""
+    import xml.etree.ElementTree as ET
+    import how_mhd as hm
+    prob, n, bc, parts = case
+    kw = dict(nx=n[0], ny=n[1], nz=n[2], nt=1, tend=0.1, gam=5.0 / 3.0, cour=0.4, problem=prob,
+              x1bc=bc[0], x2bc=bc[1], x3bc=bc[2], output_format=fmt)
+    p = hm.make_parameters(**kw)
+    step, time = 12, 0.0421
+    q = _state(hm, p, 5)
+    with hm.Group(p, parts) as g:
+        g.set_state(q)
+        master, pieces = g.output(step, time, tmp_path / "ours")
+        ranges = [g.part_range(k) for k in range(parts)]
+    inp = write_input(tmp_path / "in.in", **kw)
+    ext = "dat" if fmt == "dat" else "vts"
+    for r, (k0, nzl) in enumerate(ranges):
+        assert Path(pieces[r]).name == f"dump{step:06d}_rank{r:06d}.{ext}"
+        work = tmp_path / f"ref{r}"
+        work.mkdir()
+        write_dump(work / "state.bin", {"q": q[:, :, :, k0:k0 + nzl + 6]})
+        subprocess.run([str(REF_BIN), str(inp), "/dev/null", "--state", str(work / "state.bin"),
+                        "--piece", str(r), str(nzl), str(k0), "--output", str(step), repr(time)],
+                       cwd=work, check=True, capture_output=True, timeout=600)
+        ref = (work / "output" / f"dump{step:06d}.{ext}").read_bytes()
+        assert Path(pieces[r]).read_bytes() == ref, r
+    if fmt == "dat":
+        assert master is None
+        return
+    root = ET.parse(master).getroot()
+    assert root.get("type") == "PStructuredGrid"
+    grid = root.find("PStructuredGrid")
+    assert grid.get("WholeExtent") == f"0 {n[0] - 1} 0 {n[1] - 1} 0 {n[2] - 1}"
+    got = [(pc.get("Extent"), pc.get("Source")) for pc in grid.findall("Piece")]
+    want = [(f"0 {n[0] - 1} 0 {n[1] - 1} {k0} {k0 + nzl - 1}", f"dump{step:06d}_rank{r:06d}.vts")
+            for r, (k0, nzl) in enumerate(ranges)]
+    assert got == want
+    # the master declares the arrays each piece holds, in the pieces' order
+    piece = ET.fromstring(Path(pieces[0]).read_bytes().split(b"<AppendedData")[0] + b"</VTKFile>")
+    names = [a.get("Name") for a in piece.iter("DataArray") if a.get("format") == "appended" and a.get("Name")]
+    assert [a.get("Name") for a in grid.find("PPointData")] == names

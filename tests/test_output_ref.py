@@ -22,13 +22,15 @@ def _bc_index(idx, lo, hi, periodic):
     return np.clip(idx, lo, hi)
 
 
-def _expected(q, n, per, size, gam):
-    """Per-cell quantities of src/output.cpp:110-187, x fastest."""
+def _expected(q, n, per, size, gam, gn=None, kofs=0):
+    """Per-cell quantities of src/output.cpp:110-187, x fastest, for a block
+    of n cells starting at global plane kofs of a gn grid (default: n, 0)."""
     nx, ny, nz = n
+    gn = n if gn is None else gn
     i = np.arange(3, nx + 3)[None, None, :]
     j = np.arange(3, ny + 3)[None, :, None]
     k = np.arange(3, nz + 3)[:, None, None]
-    d = [size[a] / n[a] for a in range(3)]
+    d = [size[a] / gn[a] for a in range(3)]
     A = lambda v: q[v][3:nx + 3, 3:ny + 3, 3:nz + 3].transpose(2, 1, 0)   # (k, j, i)
     rho, Mx, My, Mz, Bx, By, Bz, E = (A(v) for v in range(8))
     vx, vy, vz = Mx / rho, My / rho, Mz / rho
@@ -51,7 +53,7 @@ def _expected(q, n, per, size, gam):
         divB = divB + np.where(edge, diff / d[ax], diff / (2.0 * d[ax]))
     x = (np.arange(nx) + 0.5) * d[0]
     y = (np.arange(ny) + 0.5) * d[1]
-    z = (np.arange(nz) + 0.5) * d[2]
+    z = ((kofs + np.arange(nz)).astype(np.float64) + 0.5) * d[2]
     X, Y, Z = np.broadcast_arrays(x[None, None, :], y[None, :, None], z[:, None, None])
     vec = lambda a, b, c: np.stack([a, b, c], axis=-1).reshape(-1)
     return [rho.reshape(-1), pg.reshape(-1), E.reshape(-1), vv2.reshape(-1), BB2.reshape(-1),
@@ -110,3 +112,36 @@ def test_reference_dat_rows(tmp_path):
         f = row.split(" ")
         assert len(f) == 22
         assert f[9] == "%.15e" % rho[r] and f[17] == "%.15e" % pg[r] and f[21] == "%.15e" % divB[r]
+
+
+@needs_ref
+@pytest.mark.parametrize("zbc", ["periodic", "open"])
+def test_reference_piece_of_a_z_slab(tmp_path, zbc):
+    """--piece R NZ KS runs the reference's writer with the local sizes and
+    offsets an MPI rank of a z-split holds: the header names the rank, the
+    global extent, the piece's extent and its global start; coordinates are
+    global; the divB diagnostic wraps (or clamps) at the slab's own edges."""
+    gn, r, k0, nzl = (6, 5, 9), 1, 4, 3
+    q = _random_state(gn, 7)
+    slab = q[:, :, :, k0:k0 + nzl + 6]
+    bc = ("periodic", "open", zbc)
+    kw = dict(nx=gn[0], ny=gn[1], nz=gn[2], nt=1, tend=0.1, gam=5.0 / 3.0, cour=0.4, problem="orszag_tang",
+              x1bc=bc[0], x2bc=bc[1], x3bc=bc[2], output_format="vts")
+    inp = write_input(tmp_path / "in.in", **kw)
+    write_dump(tmp_path / "state.bin", {"q": slab})
+    subprocess.run([str(REF_BIN), str(inp), "/dev/null", "--state", str(tmp_path / "state.bin"),
+                    "--piece", str(r), str(nzl), str(k0), "--output", "5", "0.25"], cwd=tmp_path, check=True,
+                   capture_output=True, timeout=300)
+    raw = (tmp_path / "output" / "dump000005.vts").read_bytes()
+    head, _, rest = raw.partition(b'<AppendedData encoding="raw">\n_')
+    assert b'WholeExtent="0 5 0 4 0 8"' in head
+    assert b'<Piece Extent="0 5 0 4 4 6">' in head
+    assert b'Name="rank" NumberOfTuples="1" format="ascii">\n          1\n' in head
+    assert b'format="ascii">\n          0 0 4\n' in head
+    offs = [int(t.split(b'"')[0]) for t in head.split(b'offset="')[1:]]
+    per = [b == "periodic" for b in bc]
+    exp = _expected(slab, (gn[0], gn[1], nzl), per, (1.0, 1.0, 1.0), 5.0 / 3.0, gn=gn, kofs=k0)
+    for off, e in zip(offs, exp):
+        (nbytes,) = struct.unpack("<Q", rest[off:off + 8])
+        got = np.frombuffer(rest[off + 8:off + 8 + nbytes], dtype="<f8")
+        np.testing.assert_array_equal(got.view(np.uint64), e.astype("<f8").view(np.uint64))
