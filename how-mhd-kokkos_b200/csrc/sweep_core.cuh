@@ -170,9 +170,11 @@ __device__ __forceinline__ R eig_col_sign(int m, const R* S) {
 template <typename R, int NI>
 __device__ __forceinline__ void eig_left_row(int m, const R* S, R gam0, R gam1, R* L) {
     if (m == 3) {
-        const R ics2 = S[S_ICS2 * NI], cs2 = S[S_CS2 * NI], vv2 = S[S_VV2 * NI];
+        // row (-c^2/gam0 - v^2/2, v, B_t, -1) times s = -gam0/c^2; its first
+        // entry (-c^2/gam0 - v^2/2) s = 1 - (v^2/2) s needs no division
+        const R ics2 = S[S_ICS2 * NI], vv2 = S[S_VV2 * NI];
         const R s = -gam0 * ics2;
-        L[0] = (-cs2 / gam0 - R(0.5) * vv2) * s;
+        L[0] = R(1) - R(0.5) * vv2 * s;
         L[1] = S[S_VX * NI] * s; L[2] = S[S_VY * NI] * s; L[3] = S[S_VZ * NI] * s;
         L[4] = S[S_BY * NI] * s; L[5] = S[S_BZ * NI] * s; L[6] = -s;
     } else if (m == 1 || m == 5) {

@@ -121,7 +121,9 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     // collection runs the FP64 method
     // Blocks per SM (the launch bound that caps registers): six for the plain
     // FP64 sweep (80 registers, one interface per thread in P3), seven for
-    // the mixed ones (72 registers); measured at 256^3 against 4/5 and 6/8.
+    // the learned one (72 registers), six for the plain mixed one (80
+    // registers, no spills); measured at 256^3 against 4/5 and 6/8 (FP64),
+    // 6 (learned) and 7 (plain mixed).
 #define HOW_SWEEP_CASES(D)                                                                              \
     do {                                                                                                \
         using S = SweepShape<D>;                                                                        \
@@ -129,7 +131,7 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
         if (mixed) {                                                                                    \
             if (mode == 1) launch_one<D, S::NL, S::T, 128, float, 7, 1>(c, a);                          \
             else if (mode == 2) launch_one<D, S::NL, S::T, 128, float, 5, 2>(c, a);                     \
-            else launch_one<D, S::NL, S::T, 128, float, 7, 0>(c, a);                                    \
+            else launch_one<D, S::NL, S::T, 128, float, 6, 0>(c, a);                                    \
         } else {                                                                                        \
             if (mode == 1) launch_one<D, S::NL, S::T, 128, double, 3, 1>(c, a);                         \
             else if (mode == 2) launch_one<D, S::NL, S::T, 128, double, 3, 2>(c, a);                    \
