@@ -675,6 +675,7 @@ def bench_accuracy(args):
     w, thr = hm.default_router()
     forms = [("fp64", "fp64", None, 5), ("mixed", "mixed", None, 5), ("mixed+learned", "mixed", "learned", 5),
              ("mixed+learned, decisions every stage", "mixed", "learned", 1),
+             ("mixed+learned, decisions every two steps", "mixed", "learned", 10),
              ("mixed+guard", "mixed", "guard", 5)]
     if args.forms:
         keep = {f.strip() for f in args.forms.split(";")}

@@ -78,6 +78,12 @@ void stage_sweeps(Ctx& c, int iw) {
     const double c4 = iw == 5 ? k.k4 / k.k1 : 0.0;
     const double c5 = iw == 5 ? k.k5 / k.k1 : 0.0;
     const int stage5 = iw == 5;
+    // learned routing: fresh decisions at a step's first stage and then every
+    // route_refresh stages within the step (1..5), or at the first stage of
+    // every second step (10); always when the arrays do not hold this run's
+    if (!c.route_valid) c.route_age = 0;
+    c.route_due = !c.route_valid ||
+                  (c.route_refresh <= 5 ? (iw - 1) % c.route_refresh == 0 : c.route_age % c.route_refresh == 0);
     SweepArgs a;
     a.g = g;
     a.qprev = c.q[iw - 1];
@@ -111,6 +117,11 @@ void stage_sweeps(Ctx& c, int iw) {
     if (first) {
         // no sweep at all (1x1x1): q(iw) = base
         launch_copy_fields(c, c.q[iw], c.q[0], 8);
+    }
+    if (c.route_mode == 1 && !first) {
+        if (c.route_due) c.route_age = 0;
+        c.route_valid = true;
+        ++c.route_age;
     }
 }
 
@@ -263,6 +274,7 @@ int how_set_state(how_ctx* c, int stage, const double* q) {
     HOW_CUDA_CHECK(cudaMemcpyAsync(c->stage_buf, q, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     launch_ref_to_dev(*c, c->stage_buf, c->q[stage], 8);
     if (stage == 0) c->have_state = true;
+    c->route_valid = false;   // routing decisions are of the previous state
     return sync_and_status(*c);
 }
 
@@ -354,6 +366,7 @@ int how_init_problem(how_ctx* c) {
     launch_bound(*c, f, 8);
     launch_init_faceb(*c);
     c->have_state = true;
+    c->route_valid = false;
     return sync_and_status(*c);
 }
 
@@ -400,6 +413,8 @@ int how_sweep(how_ctx* c, int dir, double dt) {
     if (n <= 1) { set_error("no sweep along an axis with one cell"); return HOW_ERR_ARG; }
     if ((rc = upload_dt(c, dt))) return rc;
     c->cur_stage = 1;
+    c->route_valid = false;   // a lone sweep routes from its own state
+    c->route_due = true;
     // stage 1: copy_stage(q, 1, 0), copy_bfield_stage(1, 0), then the sweep
     // (src/ssprk.cpp:1288-1289, 1306-1317)
     launch_copy_fields(*c, c->q[1], c->q[0], 8);

@@ -173,8 +173,15 @@ struct Ctx {
     unsigned int* collect_n = nullptr;
     unsigned int collect_cap = 0, collect_every = 1;
     float route_thr = 0.0f, guard_jump = 0.25f, guard_floor = 100.0f;
-    int route_refresh = 5;                // learned routing: fresh decisions every this many stages (1..5)
+    int route_refresh = 5;                // learned routing: fresh decisions every this many stages (1..5, 10)
     int cur_stage = 1;                    // SSPRK stage being launched (1..5)
+    // learned routing: whether the decision arrays hold the network's
+    // decisions for the current run (cleared by any change of the state or
+    // of the router), stages since they were formed, and whether the stage
+    // being launched forms fresh ones
+    bool route_valid = false;
+    long long route_age = 0;
+    bool route_due = true;
     int wait_expire = 0;                  // failure-detection test hook (SweepArgs::wait_expire)
     // part of a domain decomposed into z slabs (how_group_*): the global z
     // index of local plane 3 minus 3, and which z ghost layers this context

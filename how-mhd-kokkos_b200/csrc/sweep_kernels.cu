@@ -106,11 +106,11 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     const bool mixed = c.precision == HOW_PREC_MIXED;
     const int mode = c.route_mode;
     if (mode == 1) {
-        // learned routing: the routing pass forms fresh decisions (every
-        // route_refresh stages, starting at a step's first) into the other half of this
+        // learned routing: the routing pass forms fresh decisions (on the
+        // stages stage_sweeps marks due) into the other half of this
         // direction's pair, which then becomes the current one; the sweep
         // reads the current decisions
-        if ((c.cur_stage - 1) % c.route_refresh == 0) {
+        if (c.route_due) {
             launch_route(c, dir, a.qprev, a.route_prev, a.route_next);
             c.route_par[dir] ^= 1;
         }
@@ -141,7 +141,11 @@ void launch_sweep(Ctx& c, int dir, const SweepArgs& a_in) {
     if (dir == 0) HOW_SWEEP_CASES(0);
     else if (dir == 1) HOW_SWEEP_CASES(1);
     else HOW_SWEEP_CASES(2);
-    if (mode == 2 || mode == 3) c.route_par[dir] ^= 1;
+    if (mode == 2 || mode == 3) {
+        // guard-only routing and label collection write the decision arrays
+        c.route_par[dir] ^= 1;
+        c.route_valid = false;
+    }
 #undef HOW_SWEEP_CASES
 }
 

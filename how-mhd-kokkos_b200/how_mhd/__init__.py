@@ -430,8 +430,9 @@ class Domain:
 
     def set_router_refresh(self, stages):
         """Learned routing: the network's decisions every `stages` SSPRK
-        stages (5 = once per step, the default; 1 = every stage); the guard is
-        evaluated at every stage."""
+        stages of a step (5 = once per step, the default; 1 = every stage), or
+        with 10 once every second step; the guard is evaluated at every
+        stage."""
         _check(_lib.how_router_set_refresh(self._h, int(stages)))
 
     def router_stats(self, reset=False, groups=False):

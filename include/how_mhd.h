@@ -270,9 +270,11 @@ int how_router_default(float* w, int n, float* threshold);
 int how_router_set_weights(how_ctx* ctx, const float* w, int n);
 /* mode 0 off, 1 network + guard, 2 guard only; full WENO when logit > threshold */
 int how_router_configure(how_ctx* ctx, int mode, float threshold, float guard_jump, float guard_floor);
-/* mode 1: the network's decisions are formed every `stages` SSPRK stages
- * (5 = once per step, the default; 1 = every stage) and reused by the sweeps
- * in between; the hard guard is evaluated at every stage in any case */
+/* mode 1: the network's decisions are formed every `stages` SSPRK stages of
+ * a step from its first (5 = once per step, the default; 1 = every stage), or
+ * with 10 at the first stage of every second step, and reused by the sweeps
+ * in between; the hard guard is evaluated at every stage in any case.  Any
+ * change of the state or of the router makes the next stage form fresh ones. */
 int how_router_set_refresh(how_ctx* ctx, int stages);
 int how_router_stats(how_ctx* ctx, unsigned long long* full, unsigned long long* cheap, int reset);
 /* ... plus the 16-interface groups whose logits came from the tensor cores and

@@ -193,3 +193,36 @@ def test_router_on_key_uses_builtin_network():
         d.run(0.0, 3)
         full, cheap, mma, flat = d.router_stats(groups=True)
     assert full > 0 and cheap > 0 and mma + flat > 0
+
+
+def test_refresh_every_two_steps():
+    """Decisions formed once every two steps (refresh 10) on the magnetised
+    blast 64^3 to t = 0.2: within the same density bar as once per step, with
+    half the routing passes; a state change in between forms fresh ones."""
+    import how_mhd as hm
+    w, thr = hm.default_router()
+    ref, _ = _blast_final(64, 0.2, "fp64")
+    p = hm.make_parameters(nx=64, ny=64, nz=64, nt=1, tend=0.2, gam=5.0 / 3.0, cour=0.4, problem="blast3d_b",
+                           rhomin=1e-6, pgmin=1e-6, precision="mixed")
+    with hm.Domain(p) as d:
+        d.init_problem()
+        d.set_router(w, "learned", threshold=thr)
+        d.set_router_refresh(10)
+        l0 = d.kernel_launches
+        t4, _, _ = d.run(0.0, 4)
+        launches4 = d.kernel_launches - l0
+        d.run(t4, -1)
+        got = active(d.get_state(0), 64, 64, 64)[0]
+    with hm.Domain(p) as d:
+        d.init_problem()
+        d.set_router(w, "learned", threshold=thr)
+        l0 = d.kernel_launches
+        d.run(0.0, 4)
+        launches4_step = d.kernel_launches - l0
+    # two routing passes (3 launches each) fewer over four steps
+    assert launches4_step - launches4 == 2 * 3, (launches4_step, launches4)
+    e = float(np.abs(got - ref).sum() / np.abs(ref).sum())
+    assert e <= 1e-5, e
+    with pytest.raises(Exception):
+        with hm.Domain(p) as d:
+            d.set_router_refresh(7)
