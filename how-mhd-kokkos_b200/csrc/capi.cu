@@ -4,6 +4,8 @@
 #include "how_internal.cuh"
 #include "tma.cuh"
 
+#include <nvtx3/nvToolsExt.h>   // header-only NVTX: named ranges for profilers, no cost without one
+
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -126,6 +128,8 @@ void stage_sweeps(Ctx& c, int iw) {
 }
 
 static void run_stage(Ctx& c, int iw) {
+    static const char* const kStageName[6] = {"", "stage 1", "stage 2", "stage 3", "stage 4", "stage 5"};
+    nvtxRangePushA(kStageName[iw]);
     const Grid& g = c.g;
     stage_sweeps(c, iw);
     const RKCoeff k = rk_coeff(iw);
@@ -142,10 +146,13 @@ static void run_stage(Ctx& c, int iw) {
     double* qf[8];
     for (int v = 0; v < 8; ++v) qf[v] = c.q[iw] + v * g.fs;
     launch_bound(c, qf, 8);
+    nvtxRangePop();
 }
 
 static void run_ssprk(Ctx& c) {
+    nvtxRangePushA("ssprk");
     for (int iw = 1; iw <= 5; ++iw) run_stage(c, iw);
+    nvtxRangePop();
     // copy_stage(q, 0, 5); copy_bfield_to_stage0 (src/ssprk.cpp:1327-1328): swap
     std::swap(c.q[0], c.q[5]);
     std::swap(c.b[0], c.b[5]);
@@ -473,8 +480,12 @@ int how_run(how_ctx* c, double* time, long max_steps, long* steps, double* dts, 
         const double target = dtout * (double)out_step;
         while (*time < target) {
             if (max_steps >= 0 && taken >= max_steps) { *steps += taken; return HOW_OK; }
+            nvtxRangePushA("tstep");
             launch_tstep(*c, *time, target, 1);
-            HOW_CUDA_CHECK(cudaMemcpyAsync(c->hsc, c->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+            const cudaError_t ce =
+                cudaMemcpyAsync(c->hsc, c->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream);
+            nvtxRangePop();
+            HOW_CUDA_CHECK(ce);
             rc = sync_and_status(*c);
             if (rc) { *steps += taken; return rc; }
             const double dt = c->hsc->dt;
